@@ -1,0 +1,147 @@
+/*
+ * swb200.h -- C ABI of the B200-native Smith-Waterman / Gotoh local-alignment
+ * library (libswb200.so), a drop-in for the alignment path of SWalign
+ * (Sterbic/Projekt-2012).
+ *
+ * Conventions shared by every entry point
+ *   - Plain C types, caller-owned inputs, no CUDA or C++ types in signatures.
+ *   - Every call returns an int status (SWB_OK = 0 or a SWB_E* code) and never
+ *     exits the process; swb_last_error() gives a one-line reason.
+ *   - Orientation is the reference's: the longer sequence is the "rows"
+ *     sequence (the reference's `first` after the swap in src/SWutils.cpp:83-88;
+ *     equal lengths keep argument order), the shorter one the "cols" sequence.
+ *     Coordinates are 0-based (row in rows sequence, col in cols sequence); the
+ *     CLI prints the end cell 1-based like src/main.cu:224.
+ *   - Scores are exact int32.  Bytes are compared as they are (any byte value).
+ *   - One context per host thread; a context owns one CUDA device and its
+ *     buffers, which it reuses from call to call.
+ */
+#ifndef SWB200_H_
+#define SWB200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define SWB_OK            0
+#define SWB_EINVAL        1  /* bad argument (the reference exits -1 for these)   */
+#define SWB_ENOMEM        2  /* host or device allocation failed                  */
+#define SWB_ENOMEM_BUDGET 3  /* request does not fit the context's HBM budget     */
+#define SWB_ETIMEOUT      4  /* a bounded device wait ran out                      */
+#define SWB_ECUDA         5  /* CUDA runtime error (the reference exits -2)        */
+#define SWB_EUNSUPPORTED  6  /* size or option outside what this build supports   */
+#define SWB_EBUSY         7  /* queue full / request slot unavailable              */
+#define SWB_ENOTFOUND     8  /* unknown request id                                 */
+
+/* ---------------------------------------------------------------- types */
+
+/* Replaces `scoring` (src/SWutils.h:15-20; `first` = gap_open).  A gap of
+ * length L costs gap_open + (L-1)*gap_extend (src/FindAlignment.cuh:54-56). */
+typedef struct {
+    int32_t match;
+    int32_t mismatch;
+    int32_t gap_open;
+    int32_t gap_extend;
+} swb_scoring;
+
+/* Replaces `TracebackScore` (src/SWutils.h:34-39): a cell where the alignment
+ * crosses a special row.  gap = 1 when the path crosses that row inside a
+ * vertical gap; score is the forward value of the path's state at that cell. */
+typedef struct {
+    int32_t gap;
+    int32_t score;
+    int64_t row;
+    int64_t col;
+} swb_xpoint;
+
+/* Tie rule among cells that share the best score. */
+#define SWB_TIE_REFERENCE 0u   /* the shipped reference's thread-ownership order  */
+#define SWB_TIE_ROWMAJOR  1u   /* first cell in row-major order                   */
+
+/* Flags for swb_align_pair / swb_align_pair_device. */
+#define SWB_FLAG_TIE_ROWMAJOR  0x1u  /* default is SWB_TIE_REFERENCE              */
+#define SWB_FLAG_SCORE_ONLY    0x2u  /* score and end cell only (stage 1)          */
+#define SWB_FLAG_NO_SPECIAL    0x4u  /* stage 1 without special-row checkpoints    */
+
+typedef struct {
+    int32_t score;
+    int64_t end_row, end_col;       /* 0-based; (0,0) when the best score is 0      */
+    int64_t start_row, start_col;   /* first aligned cell; = end when score-only    */
+    int32_t swapped;                /* 1: argument A was shorter and became cols    */
+    int64_t rows, cols;             /* lengths in the rows / cols orientation       */
+    double  stage1_ms;              /* device time of the scoring wavefront         */
+    double  stage2_ms;              /* device + host time of traceback              */
+    double  total_ms;               /* wall time of the call                        */
+    /* alignment, library-owned until swb_result_free(): ops[i] in {'M','I','D'}
+     * from start to end.  'M' aligns rows[r] with cols[c]; 'I' is cols[c]
+     * against a gap; 'D' is rows[r] against a gap. */
+    int64_t n_ops;
+    char   *ops;
+    /* crosspoints in the reference's output order (src/main.cu:245-248):
+     * [start (score 0), one per special row of height xpoint_interval crossed,
+     *  end (best score)]; library-owned until swb_result_free(). */
+    int64_t     n_xpoints;
+    swb_xpoint *xpoints;
+    int32_t     xpoint_interval;    /* rows between reference special rows (4*T)    */
+    int32_t     special_interval;   /* rows between this run's HBM special rows     */
+    int64_t     special_bytes;      /* HBM held by special rows for this call       */
+} swb_result;
+
+typedef struct {
+    int32_t  device;                /* CUDA device ordinal                           */
+    uint64_t hbm_budget_bytes;      /* cap on special rows + sequences; 0 = 40 GiB  */
+    int32_t  special_interval;      /* special-row spacing in rows; 0 = autotune    */
+    int32_t  verbose;               /* nonzero: progress lines on stderr             */
+} swb_options;
+
+typedef struct swb_ctx swb_ctx;
+
+/* ---------------------------------------------------------------- calls */
+
+void swb_options_default(swb_options *opts);
+
+/* Creates a context on opts->device (opts may be NULL for defaults). */
+int swb_ctx_create(const swb_options *opts, swb_ctx **out);
+void swb_ctx_destroy(swb_ctx *ctx);
+
+/* Last error message of the context (or of the thread when ctx is NULL). */
+const char *swb_last_error(const swb_ctx *ctx);
+
+/* Replaces initScoringValues (src/SWutils.cpp:26-47): parses with atoi and
+ * rejects match < 1 or mismatch/gap_open/gap_extend > -1 with SWB_EINVAL. */
+int swb_scoring_parse(const char *match, const char *mismatch, const char *gap_open,
+                      const char *gap_extend, swb_scoring *out);
+
+/* Replaces the reference's stage-1 dk loop (src/main.cu:161-214) and its
+ * stage 2 (src/Crosspointer.cpp:104-338, driven through kernelWrapperTB,
+ * src/main.cu:17-100): aligns host sequences a (length la) and b (length lb).
+ * The longer one becomes rows.  Result buffers are library-owned; release them
+ * with swb_result_free(). */
+int swb_align_pair(swb_ctx *ctx, const uint8_t *a, int64_t la, const uint8_t *b, int64_t lb,
+                   const swb_scoring *sc, uint32_t flags, swb_result *out);
+
+/* Same as swb_align_pair but with the sequences already in device memory of the
+ * context's device (d_rows is the longer sequence, d_cols the shorter one;
+ * rows >= cols is required). */
+int swb_align_pair_device(swb_ctx *ctx, const void *d_rows, int64_t rows, const void *d_cols,
+                          int64_t cols, const swb_scoring *sc, uint32_t flags, swb_result *out);
+
+void swb_result_free(swb_result *res);
+
+/* Reference launch shape and padding for lengths (rows >= cols):
+ * src/SWutils.cpp:233-253 and src/FASTA.cpp:107-134.  Returns SWB_EUNSUPPORTED
+ * when the reference could not launch (cols < 4). */
+int swb_reference_geometry(int64_t rows, int64_t cols, int32_t *G, int32_t *T, int64_t *P1,
+                           int64_t *P2);
+
+/* Library version string. */
+const char *swb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

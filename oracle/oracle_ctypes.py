@@ -1,0 +1,187 @@
+"""ctypes access to the CPU oracle (oracle/build/liboracle.so) and to the CPU
+build of the reference (oracle/_ref/swalign_emu).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline / reference legs, never by the product.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "build", "liboracle.so")
+REFEMU_PATH = os.path.join(HERE, "_ref", "swalign_emu")
+
+TEXTBOOK, SHIPPED_CARRY = 0, 1
+TIE_REFERENCE, TIE_ROWMAJOR = 0, 1
+
+
+class Scoring(C.Structure):
+    _fields_ = [("match", C.c_int32), ("mismatch", C.c_int32),
+                ("gap_open", C.c_int32), ("gap_extend", C.c_int32)]
+
+
+class Geom(C.Structure):
+    _fields_ = [("G", C.c_int32), ("T", C.c_int32), ("P1", C.c_int64),
+                ("P2", C.c_int64), ("C", C.c_int64)]
+
+
+class End(C.Structure):
+    _fields_ = [("score", C.c_int32), ("row", C.c_int64), ("col", C.c_int64)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            subprocess.run(["make", "-C", HERE, "build/liboracle.so"], check=True,
+                           stdout=subprocess.DEVNULL)
+        L = C.CDLL(LIB_PATH)
+        u8p = C.c_char_p
+        L.orc_geometry.argtypes = [C.c_int64, C.c_int64, C.POINTER(Geom)]
+        L.orc_geometry.restype = C.c_int
+        L.orc_tie_key.argtypes = [C.POINTER(Geom), C.c_int, C.c_int64, C.c_int64]
+        L.orc_tie_key.restype = C.c_uint64
+        L.orc_stage1.argtypes = [u8p, C.c_int64, u8p, C.c_int64, C.POINTER(Scoring),
+                                 C.c_int, C.c_int, C.POINTER(End)]
+        L.orc_stage1.restype = C.c_int
+        L.orc_stage1_mt.argtypes = [u8p, C.c_int64, u8p, C.c_int64, C.POINTER(Scoring),
+                                    C.c_int, C.c_int, C.POINTER(End), C.POINTER(C.c_int64)]
+        L.orc_stage1_mt.restype = C.c_int
+        L.orc_special_rows.argtypes = [u8p, C.c_int64, u8p, C.c_int64, C.POINTER(Scoring),
+                                       C.c_int64, C.c_void_p, C.c_int64]
+        L.orc_special_rows.restype = C.c_int64
+        L.orc_traceback.argtypes = [u8p, C.c_int64, u8p, C.c_int64, C.POINTER(Scoring),
+                                    C.c_int64, C.c_int64, C.c_char_p, C.c_int64,
+                                    C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.orc_traceback.restype = C.c_int64
+        L.orc_score_ops.argtypes = [u8p, u8p, C.POINTER(Scoring), C.c_int64, C.c_int64,
+                                    C.c_char_p, C.c_int64]
+        L.orc_score_ops.restype = C.c_int64
+        _lib = L
+    return _lib
+
+
+def scoring(match, mismatch, gap_open, gap_extend) -> Scoring:
+    return Scoring(match, mismatch, gap_open, gap_extend)
+
+
+def orient(a: bytes, b: bytes):
+    """Longer sequence on rows; equal lengths keep argument order (SWutils.cpp:84-88)."""
+    if len(a) < len(b):
+        return b, a, True
+    return a, b, False
+
+
+def geometry(rows: int, cols: int) -> Geom:
+    g = Geom()
+    lib().orc_geometry(rows, cols, C.byref(g))
+    return g
+
+
+@dataclass
+class Stage1:
+    score: int
+    row: int
+    col: int
+
+
+def stage1(rows: bytes, cols: bytes, sc: Scoring, semantics=TEXTBOOK, tie=TIE_REFERENCE) -> Stage1:
+    e = End()
+    rc = lib().orc_stage1(rows, len(rows), cols, len(cols), C.byref(sc), semantics, tie, C.byref(e))
+    if rc != 0:
+        raise RuntimeError(f"orc_stage1 failed: {rc}")
+    return Stage1(e.score, e.row, e.col)
+
+
+def stage1_mt(rows: bytes, cols: bytes, sc: Scoring, tie=TIE_REFERENCE, threads=None):
+    """Returns (Stage1, seconds)."""
+    threads = threads or os.cpu_count() or 1
+    e = End()
+    ns = C.c_int64(0)
+    rc = lib().orc_stage1_mt(rows, len(rows), cols, len(cols), C.byref(sc), tie, threads,
+                             C.byref(e), C.byref(ns))
+    if rc != 0:
+        raise RuntimeError(f"orc_stage1_mt failed: {rc}")
+    return Stage1(e.score, e.row, e.col), ns.value * 1e-9
+
+
+def special_rows(rows: bytes, cols: bytes, sc: Scoring, k: int):
+    import numpy as np
+    nrows = len(rows) // k
+    out = np.zeros((max(nrows, 1), len(cols), 2), dtype=np.int32)
+    got = lib().orc_special_rows(rows, len(rows), cols, len(cols), C.byref(sc), k,
+                                 out.ctypes.data, nrows)
+    return out[:got]
+
+
+def traceback(rows: bytes, cols: bytes, sc: Scoring, er: int, ec: int):
+    """Returns (ops:str, start_row, start_col)."""
+    cap = len(rows) + len(cols) + 8
+    buf = C.create_string_buffer(cap)
+    sr, scol = C.c_int64(0), C.c_int64(0)
+    k = lib().orc_traceback(rows, len(rows), cols, len(cols), C.byref(sc), er, ec, buf, cap,
+                            C.byref(sr), C.byref(scol))
+    if k < 0:
+        raise RuntimeError(f"orc_traceback failed: {k}")
+    return buf.raw[:k].decode(), sr.value, scol.value
+
+
+def score_ops(rows: bytes, cols: bytes, sc: Scoring, sr: int, scol: int, ops: str) -> int:
+    o = ops.encode()
+    return lib().orc_score_ops(rows, cols, C.byref(sc), sr, scol, o, len(o))
+
+
+def crosspoints(ops: str, sr: int, scol: int, interval: int):
+    """Rows where the path leaves a special row (0-based R = interval*k - 1) going
+    down: returns [(row, col)] for each special row the path crosses, top to bottom."""
+    out = []
+    r, c = sr, scol
+    path = [(r, c)]
+    for o in ops[1:]:
+        if o == "M":
+            r += 1; c += 1
+        elif o == "I":
+            c += 1
+        else:
+            r += 1
+        path.append((r, c))
+    last_in_row = {}
+    for (pr, pc) in path:
+        last_in_row[pr] = pc
+    er = path[-1][0]
+    R = interval - 1
+    while R < er:
+        if R in last_in_row and R >= sr:
+            out.append((R, last_in_row[R]))
+        R += interval
+    return out
+
+
+def run_reference(fa: str, fb: str, match: int, mismatch: int, gap_open: int, gap_extend: int,
+                  stage1_only=True, timeout=600):
+    """Runs the CPU build of the reference; returns dict with score/row1/col1/geom/xpoints
+    or raises subprocess.TimeoutExpired / RuntimeError."""
+    if not os.path.exists(REFEMU_PATH):
+        raise FileNotFoundError(REFEMU_PATH)
+    args = [REFEMU_PATH, fa, fb, str(match), str(mismatch), str(gap_open), str(gap_extend)]
+    if stage1_only:
+        args.append("--stage1-only")
+    p = subprocess.run(args, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, timeout=timeout)
+    res = {"rc": p.returncode, "xpoints": []}
+    for line in p.stderr.decode(errors="replace").splitlines():
+        f = line.split()
+        if len(f) >= 2 and f[0] == "REFEMU":
+            if f[1] == "score":
+                res["score"], res["row1"], res["col1"] = int(f[2]), int(f[3]), int(f[4])
+            elif f[1] == "geom":
+                res["G"], res["T"], res["P1"], res["P2"] = map(int, f[2:6])
+            elif f[1] == "xpoint":
+                res["xpoints"].append(tuple(int(x) for x in f[3:7]))
+    return res

@@ -1,0 +1,81 @@
+/*
+ * sw_oracle.h -- CPU restatement of the reference SWalign (Sterbic/Projekt-2012)
+ * Smith-Waterman / Gotoh local-alignment path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and bench.py's
+ * CPU-baseline leg may load this library, and only as the checker or the timed
+ * CPU baseline.  The product library never links, loads or calls it.
+ *
+ * Orientation follows the reference: "rows" is the longer sequence (the
+ * reference's "first" after the swap in src/SWutils.cpp:83-88; equal lengths
+ * keep argument order), "cols" is the shorter one.  All coordinates are 0-based.
+ */
+#ifndef SW_ORACLE_H_
+#define SW_ORACLE_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {            /* src/SWutils.h:15-20 (`first` is the gap-open penalty) */
+    int32_t match, mismatch, gap_open, gap_extend;
+} orc_scoring;
+
+typedef struct {            /* launch shape + padding of the shipped reference */
+    int32_t G, T;           /* blocks, threads: src/SWutils.cpp:233-253          */
+    int64_t P1, P2, C;      /* padded rows / cols, column chunk P2/G: FASTA.cpp:107-134 */
+} orc_geom;
+
+typedef struct {
+    int32_t score;
+    int64_t row, col;       /* end cell, 0-based; (0,0) when every cell is 0      */
+} orc_end;
+
+enum { ORC_TEXTBOOK = 0,    /* zero boundaries: the H matrix of textbook Gotoh SW */
+       ORC_SHIPPED_CARRY = 1 /* the shipped kernels' left boundary carry (see .c)  */ };
+enum { ORC_TIE_REFERENCE = 0, /* the shipped kernels' thread-ownership order      */
+       ORC_TIE_ROWMAJOR = 1 };
+
+/* Returns 0, or -1 when the reference cannot launch (shorter length < 4). */
+int orc_geometry(int64_t rows, int64_t cols, orc_geom *g);
+
+/* Ordering key of cell (r, c) under the tie rule (smaller wins among equal H). */
+uint64_t orc_tie_key(const orc_geom *g, int tie, int64_t r, int64_t c);
+
+/* Stage 1: best local score and its end cell.  a = rows, b = cols (|a| >= |b|). */
+int orc_stage1(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
+               const orc_scoring *sc, int semantics, int tie, orc_end *out);
+
+/* Stage 1 on all `threads` host threads (blocked wavefront), textbook semantics.
+ * Same result as orc_stage1(..., ORC_TEXTBOOK, tie, ...).  Returns elapsed ns in
+ * *ns_out when it is not NULL. */
+int orc_stage1_mt(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
+                  const orc_scoring *sc, int tie, int threads, orc_end *out, int64_t *ns_out);
+
+/* Full H/E/F rows for checking special rows: writes H and F of every row r with
+ * (r + 1) % k == 0 into hf[(r + 1) / k - 1][c] as (H, F) pairs (textbook).
+ * Returns the number of rows written. */
+int64_t orc_special_rows(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
+                         const orc_scoring *sc, int64_t k, int32_t *hf, int64_t max_rows);
+
+/* Canonical traceback from end cell (er, ec), textbook semantics, full matrix in
+ * memory (m * n bytes).  Precedence: in H, diagonal > E (gap in rows' sequence,
+ * horizontal) > F (vertical); in E or F, extend > open.  Writes the operations
+ * from start to end into ops ('M' diagonal, 'I' horizontal = column base against
+ * a gap, 'D' vertical = row base against a gap), returns their count, and the
+ * start cell (first 'M') in *sr, *sc_.  Returns -1 if cap is too small or the
+ * matrix does not fit, -2 on bad input. */
+int64_t orc_traceback(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
+                      const orc_scoring *sc, int64_t er, int64_t ec,
+                      char *ops, int64_t cap, int64_t *sr, int64_t *sc_);
+
+/* Score of an alignment given as ops from (sr, sc_) (checks a traceback). */
+int64_t orc_score_ops(const uint8_t *a, const uint8_t *b, const orc_scoring *sc,
+                      int64_t sr, int64_t sc_, const char *ops, int64_t nops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

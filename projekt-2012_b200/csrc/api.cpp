@@ -1,0 +1,397 @@
+// api.cpp -- context, device buffers and the pair entry points of libswb200.so.
+//
+// Host orchestration that replaces src/main.cu:102-249 (load -> device ->
+// stage 1 -> reduction -> stage 2) without any process exit, file I/O or
+// per-step host round trips: the whole of stage 1 is one persistent launch and
+// the special rows stay in HBM (the reference appends them to temp/row_<R>
+// files, src/Builders.cpp:41-61).
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "swb_internal.h"
+#include "traceback.h"
+
+#define SWB_VERSION_STRING "swb200 0.1.0 (sm_100a)"
+
+namespace {
+
+thread_local std::string g_thread_err;
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = bytes < 256 ? 256 : bytes;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+}  // namespace
+
+struct swb_ctx {
+    int device = 0;
+    swb_options opts{};
+    cudaStream_t stream = nullptr;
+    int sms = 0;
+    std::string err;
+    DevBuf rows, cols, hbuf, progress, wbest, best, errf, srows, scols, work;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::mutex mu;
+    // last stage-1 special-row layout (for swb_special_row_copy)
+    int64_t last_nsr = 0, last_n = 0, last_sr_interval = 0;
+};
+
+static int fail(swb_ctx *ctx, int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->err = buf;
+    g_thread_err = buf;
+    return code;
+}
+
+static int cuda_fail(swb_ctx *ctx, cudaError_t e, const char *what) {
+    return fail(ctx, SWB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+namespace swb {
+
+static int64_t pad_len(int64_t len, int64_t parts) {
+    if (len <= 0 || parts <= 0) return len;
+    const int64_t C = (len + parts - 1) / parts;
+    if (len % C == 0) return len;
+    return len + (C - len % C);
+}
+
+bool reference_geometry(int64_t rows, int64_t cols, int32_t *G, int32_t *T, int64_t *P1, int64_t *P2) {
+    int32_t blocks = 2, threads = 5;
+    if ((int64_t)threads * blocks * 2 > cols) blocks = (int32_t)((float)cols / (float)(threads * 2));
+    if (blocks == 0) {
+        blocks = 1;
+        threads = (int32_t)(cols / 4);
+    }
+    *G = blocks;
+    *T = threads;
+    *P1 = pad_len(rows, 4);
+    *P2 = pad_len(cols, blocks);
+    return threads > 0;
+}
+
+}  // namespace swb
+
+extern "C" {
+
+void swb_options_default(swb_options *o) {
+    std::memset(o, 0, sizeof *o);
+    o->device = 0;
+    o->hbm_budget_bytes = 0;
+    o->special_interval = 0;
+    o->verbose = 0;
+}
+
+int swb_ctx_create(const swb_options *opts, swb_ctx **out) {
+    if (!out) return fail(nullptr, SWB_EINVAL, "swb_ctx_create: out is NULL");
+    *out = nullptr;
+    swb_ctx *c = new (std::nothrow) swb_ctx();
+    if (!c) return fail(nullptr, SWB_ENOMEM, "swb_ctx_create: out of host memory");
+    if (opts) c->opts = *opts;
+    else swb_options_default(&c->opts);
+    if (c->opts.hbm_budget_bytes == 0) c->opts.hbm_budget_bytes = 40ULL << 30;
+    c->device = c->opts.device;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev <= 0) {
+        delete c;
+        return fail(nullptr, SWB_ECUDA, "no CUDA device: %s", cudaGetErrorString(e));
+    }
+    if (c->device < 0 || c->device >= ndev) {
+        const int dev = c->device;
+        delete c;
+        return fail(nullptr, SWB_EINVAL, "device %d out of range (%d devices)", dev, ndev);
+    }
+    if ((e = cudaSetDevice(c->device)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess) {
+        int rc = cuda_fail(nullptr, e, "swb_ctx_create");
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return SWB_OK;
+}
+
+void swb_ctx_destroy(swb_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (DevBuf *b : {&c->rows, &c->cols, &c->hbuf, &c->progress, &c->wbest, &c->best, &c->errf, &c->srows,
+                      &c->scols, &c->work})
+        b->release();
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char *swb_last_error(const swb_ctx *c) { return c ? c->err.c_str() : g_thread_err.c_str(); }
+
+const char *swb_version(void) { return SWB_VERSION_STRING; }
+
+int swb_scoring_parse(const char *match, const char *mismatch, const char *gap_open, const char *gap_extend,
+                      swb_scoring *out) {
+    if (!match || !mismatch || !gap_open || !gap_extend || !out)
+        return fail(nullptr, SWB_EINVAL, "swb_scoring_parse: NULL argument");
+    swb_scoring s;
+    s.match = std::atoi(match);
+    s.mismatch = std::atoi(mismatch);
+    s.gap_open = std::atoi(gap_open);
+    s.gap_extend = std::atoi(gap_extend);
+    if (s.match < 1 || s.mismatch > -1 || s.gap_open > -1 || s.gap_extend > -1)
+        return fail(nullptr, SWB_EINVAL, "One or more scoring values were not usable!");
+    *out = s;
+    return SWB_OK;
+}
+
+int swb_reference_geometry(int64_t rows, int64_t cols, int32_t *G, int32_t *T, int64_t *P1, int64_t *P2) {
+    int32_t g = 0, t = 0;
+    int64_t p1 = 0, p2 = 0;
+    const bool ok = swb::reference_geometry(rows, cols, &g, &t, &p1, &p2);
+    if (G) *G = g;
+    if (T) *T = t;
+    if (P1) *P1 = p1;
+    if (P2) *P2 = p2;
+    return ok ? SWB_OK : SWB_EUNSUPPORTED;
+}
+
+void swb_result_free(swb_result *r) {
+    if (!r) return;
+    std::free(r->ops);
+    std::free(r->xpoints);
+    r->ops = nullptr;
+    r->xpoints = nullptr;
+    r->n_ops = 0;
+    r->n_xpoints = 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Scoring values must stay in the exact int32 range of the recurrence for the
+// lengths involved (|score| <= max(|s|) * (rows + cols)).
+int check_scoring(swb_ctx *c, const swb_scoring *sc, int64_t rows, int64_t cols) {
+    if (!sc) return fail(c, SWB_EINVAL, "scoring is NULL");
+    if (sc->match < 1 || sc->mismatch > -1 || sc->gap_open > -1 || sc->gap_extend > -1)
+        return fail(c, SWB_EINVAL, "One or more scoring values were not usable!");
+    const long double worst = (long double)std::max<int64_t>(
+                                  {(int64_t)sc->match, -(int64_t)sc->mismatch, -(int64_t)sc->gap_open,
+                                   -(int64_t)sc->gap_extend}) *
+                              (long double)(rows + cols + 2);
+    if (worst > 2.0e9L) return fail(c, SWB_EUNSUPPORTED, "scores would leave the int32 range");
+    return SWB_OK;
+}
+
+// Runs stage 1 on device sequences already in the context's buffers.
+int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_cols, int64_t n,
+               const swb_scoring *sc, uint32_t flags, int64_t sr_interval_rows, swb::BestRec *best_out,
+               float *ms_out, int64_t *nsr_out) {
+    using namespace swb;
+    const int R = 16;
+    Stage1Plan plan = stage1_plan(m, n, c->sms, R);
+    const int64_t W = (int64_t)plan.blocks * plan.warps_per_block;
+    cudaError_t e;
+    if ((e = c->hbuf.ensure(sizeof(int2) * (size_t)std::max<int64_t>(n, 1))) != cudaSuccess ||
+        (e = c->progress.ensure(sizeof(int32_t) * (size_t)plan.nstrips)) != cudaSuccess ||
+        (e = c->wbest.ensure(sizeof(BestRec) * (size_t)W)) != cudaSuccess ||
+        (e = c->best.ensure(sizeof(BestRec))) != cudaSuccess ||
+        (e = c->errf.ensure(2 * sizeof(int32_t))) != cudaSuccess)
+        return cuda_fail(c, e, "stage 1 buffers");
+
+    Stage1Args a{};
+    a.rows = d_rows;
+    a.cols = d_cols;
+    a.m = m;
+    a.n = n;
+    a.open = sc->gap_open;
+    a.ext = sc->gap_extend;
+    a.gx = std::max(sc->gap_open, sc->gap_extend);
+    a.mt1 = sc->match - sc->gap_open;
+    a.mm1 = sc->mismatch - sc->gap_open;
+    a.hbuf = (int2 *)c->hbuf.p;
+    a.progress = (int32_t *)c->progress.p;
+    a.nstrips = plan.nstrips;
+    a.wbest = (BestRec *)c->wbest.p;
+    a.best = (BestRec *)c->best.p;
+    a.err = (int32_t *)c->errf.p;
+    a.srows = nullptr;
+    a.sr_every = 1;
+    a.nsr = 0;
+    if (sr_interval_rows > 0) {
+        const int64_t every = std::max<int64_t>(1, sr_interval_rows / plan.strip_rows);
+        const int64_t nsr = (m / plan.strip_rows) / every;
+        if (nsr > 0) {
+            const size_t bytes = sizeof(int2) * (size_t)nsr * (size_t)n;
+            if (bytes > c->opts.hbm_budget_bytes)
+                return fail(c, SWB_ENOMEM_BUDGET, "special rows need %zu bytes > budget %llu", bytes,
+                            (unsigned long long)c->opts.hbm_budget_bytes);
+            if ((e = c->srows.ensure(bytes)) != cudaSuccess) return cuda_fail(c, e, "special rows");
+            a.srows = (int2 *)c->srows.p;
+            a.sr_every = every;
+            a.nsr = nsr;
+        }
+    }
+    c->last_nsr = a.nsr;
+    c->last_n = n;
+    c->last_sr_interval = a.nsr > 0 ? a.sr_every * plan.strip_rows : 0;
+    if (nsr_out) *nsr_out = a.nsr;
+    int32_t G = 0, T = 0;
+    int64_t P1 = 0, P2 = 0;
+    const bool refok = reference_geometry(m, n, &G, &T, &P1, &P2);
+    a.tie.mode = ((flags & SWB_FLAG_TIE_ROWMAJOR) || !refok) ? kTieRowMajor : kTieReference;
+    a.tie.G = G;
+    a.tie.T = T;
+    a.tie.C = refok ? P2 / G : 1;
+
+    if ((e = cudaMemsetAsync(a.progress, 0, sizeof(int32_t) * (size_t)plan.nstrips, c->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(a.err, 0, 2 * sizeof(int32_t), c->stream)) != cudaSuccess)
+        return cuda_fail(c, e, "stage 1 reset");
+    cudaEventRecord(c->ev0, c->stream);
+    if ((e = stage1_launch(a, plan, c->stream)) != cudaSuccess) return cuda_fail(c, e, "stage 1 launch");
+    cudaEventRecord(c->ev1, c->stream);
+    int32_t errh[2] = {0, 0};
+    if ((e = cudaMemcpyAsync(best_out, a.best, sizeof(BestRec), cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(errh, a.err, sizeof errh, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+        return cuda_fail(c, e, "stage 1");
+    if (errh[0] != 0) return fail(c, SWB_ETIMEOUT, "stage 1: a bounded wait between strips ran out");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    if (ms_out) *ms_out = ms;
+    return SWB_OK;
+}
+
+int align_device(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_cols, int64_t n,
+                 const swb_scoring *sc, uint32_t flags, swb_result *out, int swapped,
+                 const uint8_t *h_rows, const uint8_t *h_cols) {
+    using namespace swb;
+    const auto t0 = std::chrono::steady_clock::now();
+    std::memset(out, 0, sizeof *out);
+    out->rows = m;
+    out->cols = n;
+    out->swapped = swapped;
+    int32_t G = 0, T = 0;
+    int64_t P1 = 0, P2 = 0;
+    reference_geometry(m, n, &G, &T, &P1, &P2);
+    out->xpoint_interval = T > 0 ? 4 * T : 20;
+    if (m == 0 || n == 0) {
+        out->total_ms = 0;
+        return SWB_OK;
+    }
+    const bool score_only = (flags & SWB_FLAG_SCORE_ONLY) != 0;
+    int64_t sr_interval = 0;
+    if (!(flags & SWB_FLAG_NO_SPECIAL)) sr_interval = tb::choose_special_interval(c->opts, m, n);
+    BestRec best{};
+    float ms = 0.f;
+    int64_t nsr = 0;
+    int rc = run_stage1(c, d_rows, m, d_cols, n, sc, flags, sr_interval, &best, &ms, &nsr);
+    if (rc != SWB_OK) return rc;
+    out->stage1_ms = ms;
+    out->special_interval = (int32_t)c->last_sr_interval;
+    out->special_bytes = (int64_t)sizeof(int2) * nsr * n;
+    if (best.valid) {
+        out->score = best.ho - sc->gap_open;
+        out->end_row = best.row;
+        out->end_col = best.col;
+    } else {
+        out->score = 0;
+        out->end_row = 0;
+        out->end_col = 0;
+    }
+    out->start_row = out->end_row;
+    out->start_col = out->end_col;
+    if (!score_only && out->score > 0) {
+        const auto t1 = std::chrono::steady_clock::now();
+        rc = tb::traceback(c->stream, d_rows, m, d_cols, n, sc, (const int2 *)c->srows.p, nsr,
+                           c->last_sr_interval, out, h_rows, h_cols, c->err);
+        if (rc != SWB_OK) return fail(c, rc, "%s", c->err.c_str());
+        out->stage2_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
+    }
+    out->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return SWB_OK;
+}
+
+}  // namespace
+
+extern "C" int swb_align_pair_device(swb_ctx *c, const void *d_rows, int64_t rows, const void *d_cols, int64_t cols,
+                                     const swb_scoring *sc, uint32_t flags, swb_result *out) {
+    if (!c || !out || rows < 0 || cols < 0 || rows < cols || (rows > 0 && !d_rows) || (cols > 0 && !d_cols))
+        return fail(c, SWB_EINVAL, "swb_align_pair_device: bad arguments");
+    if (rows > (int64_t)INT32_MAX - 64 || cols > (int64_t)INT32_MAX - 64)
+        return fail(c, SWB_EUNSUPPORTED, "sequence longer than 2^31 - 64");
+    int rc = check_scoring(c, sc, rows, cols);
+    if (rc != SWB_OK) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    return align_device(c, (const uint8_t *)d_rows, rows, (const uint8_t *)d_cols, cols, sc, flags, out, 0, nullptr,
+                        nullptr);
+}
+
+extern "C" int swb_align_pair(swb_ctx *c, const uint8_t *a, int64_t la, const uint8_t *b, int64_t lb,
+                              const swb_scoring *sc, uint32_t flags, swb_result *out) {
+    if (!c || !out || la < 0 || lb < 0 || (la > 0 && !a) || (lb > 0 && !b))
+        return fail(c, SWB_EINVAL, "swb_align_pair: bad arguments");
+    const bool swap = la < lb;  // src/SWutils.cpp:84-88
+    const uint8_t *hr = swap ? b : a;
+    const uint8_t *hc = swap ? a : b;
+    const int64_t m = swap ? lb : la, n = swap ? la : lb;
+    if (m > (int64_t)INT32_MAX - 64)
+        return fail(c, SWB_EUNSUPPORTED, "sequence longer than 2^31 - 64");
+    int rc = check_scoring(c, sc, m, n);
+    if (rc != SWB_OK) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    cudaError_t e;
+    if ((e = c->rows.ensure((size_t)m + 64)) != cudaSuccess || (e = c->cols.ensure((size_t)n + 64)) != cudaSuccess)
+        return cuda_fail(c, e, "sequence buffers");
+    if (m > 0 && (e = cudaMemcpyAsync(c->rows.p, hr, (size_t)m, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
+        return cuda_fail(c, e, "copy rows");
+    if (n > 0 && (e = cudaMemcpyAsync(c->cols.p, hc, (size_t)n, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
+        return cuda_fail(c, e, "copy cols");
+    return align_device(c, (const uint8_t *)c->rows.p, m, (const uint8_t *)c->cols.p, n, sc, flags, out, swap ? 1 : 0,
+                        hr, hc);
+}
+
+// Copies special row `idx` (row (idx+1)*interval - 1) of the last call as (H, F)
+// pairs into host memory `out` (2*cols int32).  Inspection entry for tests.
+extern "C" int swb_special_row_copy(swb_ctx *c, int64_t idx, int32_t *out, int64_t cols, int64_t *interval) {
+    if (!c || !out) return fail(c, SWB_EINVAL, "swb_special_row_copy: bad arguments");
+    if (interval) *interval = c->last_sr_interval;
+    if (idx < 0 || idx >= c->last_nsr || cols != c->last_n)
+        return fail(c, SWB_EINVAL, "special row %lld not available", (long long)idx);
+    cudaSetDevice(c->device);
+    cudaError_t e = cudaMemcpy(out, (const int2 *)c->srows.p + idx * c->last_n, sizeof(int2) * (size_t)cols,
+                               cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(c, e, "special row copy");
+    return SWB_OK;
+}

@@ -1,0 +1,80 @@
+// swb_internal.h -- internal declarations shared by the host and device sources
+// of libswb200.so.  Not part of the C ABI (include/swb200.h is).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "../../include/swb200.h"
+
+namespace swb {
+
+// Rows handled by one lane of the stage-1 wavefront.  A warp holds a strip of
+// 32 * R rows; special rows are kept at multiples of the strip height.
+constexpr int kLanes = 32;
+
+// Per-warp best cell: HO is H + gap_open (the kernel works on H + open so that
+// the F chain needs one DPX op per row), key orders equal scores.
+struct BestRec {
+    int32_t ho;
+    int32_t valid;
+    uint64_t key;
+    int64_t row;
+    int64_t col;
+};
+
+enum TieMode : int32_t { kTieReference = 0, kTieRowMajor = 1 };
+
+struct TieGeom {
+    int32_t mode;  // TieMode
+    int32_t G, T;  // reference launch shape
+    int64_t C;     // reference column chunk P2 / G
+};
+
+// Device buffers and scalars for one stage-1 launch.
+struct Stage1Args {
+    const uint8_t *rows;   // device, m bytes (longer sequence)
+    const uint8_t *cols;   // device, n bytes
+    int64_t m, n;
+    int32_t open, ext, gx; // gap_open, gap_extend, max(gap_open, gap_extend)
+    int32_t mt1, mm1;      // match - open, mismatch - open
+    int2 *hbuf;            // n entries: (H + open, F of the next row) of the last strip bottom
+    int32_t *progress;     // nstrips entries, zeroed before the launch
+    int2 *srows;           // special rows [nsr][n] of (H, F), or nullptr
+    int64_t sr_every;      // a special row every sr_every strips
+    int64_t nsr;           // number of special rows
+    int64_t nstrips;
+    BestRec *wbest;        // one per warp of the grid
+    BestRec *best;         // final reduced record
+    int32_t *err;          // [0] error code, [1] abort flag
+    TieGeom tie;
+};
+
+// Geometry of the reference's launch (src/SWutils.cpp:233-253) and padding
+// (src/FASTA.cpp:107-134).  Returns false when the reference could not launch.
+bool reference_geometry(int64_t rows, int64_t cols, int32_t *G, int32_t *T, int64_t *P1,
+                        int64_t *P2);
+
+// Stage-1 launch plan (chosen by the host for a pair).
+struct Stage1Plan {
+    int R = 16;            // rows per lane
+    int warps_per_block = 4;
+    int blocks = 0;
+    int64_t strip_rows = 0;
+    int64_t nstrips = 0;
+};
+
+// Host entry of stage 1: score and end cell, optional special rows.  All
+// pointers in `a` are device pointers owned by the caller.  Returns a CUDA
+// error (cudaSuccess on success); a bounded-wait timeout is reported through
+// a.err and *timed_out.
+cudaError_t stage1_launch(Stage1Args &a, const Stage1Plan &plan, cudaStream_t st);
+Stage1Plan stage1_plan(int64_t m, int64_t n, int device_sms, int R_hint);
+int stage1_max_blocks_per_sm(int R, int warps_per_block);
+
+uint64_t tie_key_host(const TieGeom &g, int64_t r, int64_t c);
+
+}  // namespace swb

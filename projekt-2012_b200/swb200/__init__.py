@@ -1,0 +1,213 @@
+"""Python access to libswb200.so (the C ABI in include/swb200.h).
+
+Used by the tests and bench.py.  The library is the product; this module only
+marshals arguments.  Loading fails loudly when the shared library is missing:
+there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Tuple
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "build", "libswb200.so")
+CLI_PATH = os.path.join(PKG_DIR, "build", "SWalign")
+
+SWB_OK = 0
+SWB_EINVAL = 1
+SWB_ENOMEM = 2
+SWB_ENOMEM_BUDGET = 3
+SWB_ETIMEOUT = 4
+SWB_ECUDA = 5
+SWB_EUNSUPPORTED = 6
+SWB_EBUSY = 7
+SWB_ENOTFOUND = 8
+
+FLAG_TIE_ROWMAJOR = 0x1
+FLAG_SCORE_ONLY = 0x2
+FLAG_NO_SPECIAL = 0x4
+
+
+class Scoring(C.Structure):
+    _fields_ = [("match", C.c_int32), ("mismatch", C.c_int32),
+                ("gap_open", C.c_int32), ("gap_extend", C.c_int32)]
+
+
+class XPoint(C.Structure):
+    _fields_ = [("gap", C.c_int32), ("score", C.c_int32), ("row", C.c_int64), ("col", C.c_int64)]
+
+
+class Result(C.Structure):
+    _fields_ = [("score", C.c_int32),
+                ("end_row", C.c_int64), ("end_col", C.c_int64),
+                ("start_row", C.c_int64), ("start_col", C.c_int64),
+                ("swapped", C.c_int32),
+                ("rows", C.c_int64), ("cols", C.c_int64),
+                ("stage1_ms", C.c_double), ("stage2_ms", C.c_double), ("total_ms", C.c_double),
+                ("n_ops", C.c_int64), ("ops", C.c_void_p),
+                ("n_xpoints", C.c_int64), ("xpoints", C.POINTER(XPoint)),
+                ("xpoint_interval", C.c_int32), ("special_interval", C.c_int32),
+                ("special_bytes", C.c_int64)]
+
+
+class Options(C.Structure):
+    _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64),
+                ("special_interval", C.c_int32), ("verbose", C.c_int32)]
+
+
+class SwbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"swb error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Loads libswb200.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with `make -C {PKG_DIR}` (no CPU fallback exists)")
+        L = C.CDLL(LIB_PATH)
+        L.swb_options_default.argtypes = [C.POINTER(Options)]
+        L.swb_ctx_create.argtypes = [C.POINTER(Options), C.POINTER(C.c_void_p)]
+        L.swb_ctx_create.restype = C.c_int
+        L.swb_ctx_destroy.argtypes = [C.c_void_p]
+        L.swb_last_error.argtypes = [C.c_void_p]
+        L.swb_last_error.restype = C.c_char_p
+        L.swb_scoring_parse.argtypes = [C.c_char_p] * 4 + [C.POINTER(Scoring)]
+        L.swb_scoring_parse.restype = C.c_int
+        L.swb_align_pair.argtypes = [C.c_void_p, C.c_char_p, C.c_int64, C.c_char_p, C.c_int64,
+                                     C.POINTER(Scoring), C.c_uint32, C.POINTER(Result)]
+        L.swb_align_pair.restype = C.c_int
+        L.swb_align_pair_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                            C.POINTER(Scoring), C.c_uint32, C.POINTER(Result)]
+        L.swb_align_pair_device.restype = C.c_int
+        L.swb_result_free.argtypes = [C.POINTER(Result)]
+        L.swb_reference_geometry.argtypes = [C.c_int64, C.c_int64, C.POINTER(C.c_int32),
+                                             C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                                             C.POINTER(C.c_int64)]
+        L.swb_reference_geometry.restype = C.c_int
+        L.swb_special_row_copy.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                           C.POINTER(C.c_int64)]
+        L.swb_special_row_copy.restype = C.c_int
+        L.swb_version.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def scoring(match, mismatch, gap_open, gap_extend) -> Scoring:
+    return Scoring(match, mismatch, gap_open, gap_extend)
+
+
+@dataclass
+class Alignment:
+    score: int
+    end_row: int
+    end_col: int
+    start_row: int
+    start_col: int
+    swapped: bool
+    rows: int
+    cols: int
+    stage1_ms: float
+    stage2_ms: float
+    total_ms: float
+    ops: str = ""
+    xpoints: List[Tuple[int, int, int, int]] = field(default_factory=list)  # (row, col, score, gap)
+    xpoint_interval: int = 0
+    special_interval: int = 0
+    special_bytes: int = 0
+
+
+def _convert(r: Result) -> Alignment:
+    ops = C.string_at(r.ops, r.n_ops).decode() if r.n_ops > 0 and r.ops else ""
+    xps = [(r.xpoints[i].row, r.xpoints[i].col, r.xpoints[i].score, r.xpoints[i].gap)
+           for i in range(r.n_xpoints)]
+    return Alignment(r.score, r.end_row, r.end_col, r.start_row, r.start_col, bool(r.swapped),
+                     r.rows, r.cols, r.stage1_ms, r.stage2_ms, r.total_ms, ops, xps,
+                     r.xpoint_interval, r.special_interval, r.special_bytes)
+
+
+class Context:
+    """One device context (owns a CUDA stream and reusable device buffers)."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, special_interval: int = 0):
+        L = lib()
+        o = Options()
+        L.swb_options_default(C.byref(o))
+        o.device = device
+        o.hbm_budget_bytes = hbm_budget_bytes
+        o.special_interval = special_interval
+        h = C.c_void_p()
+        rc = L.swb_ctx_create(C.byref(o), C.byref(h))
+        if rc != SWB_OK:
+            raise SwbError(rc, L.swb_last_error(None).decode())
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().swb_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _err(self, rc):
+        raise SwbError(rc, lib().swb_last_error(self._h).decode())
+
+    def align(self, a: bytes, b: bytes, sc: Scoring, flags: int = 0) -> Alignment:
+        r = Result()
+        rc = lib().swb_align_pair(self._h, a, len(a), b, len(b), C.byref(sc), flags, C.byref(r))
+        if rc != SWB_OK:
+            self._err(rc)
+        try:
+            return _convert(r)
+        finally:
+            lib().swb_result_free(C.byref(r))
+
+    def align_device(self, d_rows: int, rows: int, d_cols: int, cols: int, sc: Scoring,
+                     flags: int = 0) -> Alignment:
+        r = Result()
+        rc = lib().swb_align_pair_device(self._h, C.c_void_p(d_rows), rows, C.c_void_p(d_cols), cols,
+                                         C.byref(sc), flags, C.byref(r))
+        if rc != SWB_OK:
+            self._err(rc)
+        try:
+            return _convert(r)
+        finally:
+            lib().swb_result_free(C.byref(r))
+
+    def special_row(self, idx: int, cols: int):
+        import numpy as np
+        out = np.zeros((cols, 2), dtype=np.int32)
+        interval = C.c_int64(0)
+        rc = lib().swb_special_row_copy(self._h, idx, out.ctypes.data, cols, C.byref(interval))
+        if rc != SWB_OK:
+            self._err(rc)
+        return out, interval.value
+
+
+def reference_geometry(rows: int, cols: int):
+    G, T = C.c_int32(), C.c_int32()
+    P1, P2 = C.c_int64(), C.c_int64()
+    rc = lib().swb_reference_geometry(rows, cols, C.byref(G), C.byref(T), C.byref(P1), C.byref(P2))
+    return rc, G.value, T.value, P1.value, P2.value
+
+
+def version() -> str:
+    return lib().swb_version().decode()
