@@ -1,0 +1,310 @@
+"""Benchmark of the SW/Gotoh long-pair path on B200 (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload long|small|chromosome]
+
+A step is one full alignment of the workload pair through the library's C ABI.
+`value` is GCUPS (rows * cols / seconds) with the sequences resident in HBM,
+timed with CUDA events on the stream the library runs on; `e2e` is the same
+metric through swb_align_pair() from pinned host buffers (host->device copy of
+both sequences and the device->host read of the result inside the timed
+region).  With N > 1 every rank aligns its own replica of the pair (weak
+scaling, no collective on the data path) and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "projekt-2012_b200"))
+
+METRIC = "GCUPS (long pair, bit-exact); mixed-size pairs/s + p50/p99 latency vs plain"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["long", "long200k", "small", "chromosome"], default="long")
+    p.add_argument("--score-only", action="store_true", help="stage 1 only (diagnostics)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload(name):
+    from swb200 import synth
+    if name == "long":
+        a, b, sc = synth.long_pair()
+        desc = ("long pair: 1 Mbp iid ACGT vs its central 800 kbp (5% sub, 1% indel, geometric "
+                "mean 4) with 100 kbp random flanks; scoring 1/-3/-5/-2")
+    elif name == "long200k":
+        a, b, sc = synth.long_pair(length=200_000)
+        desc = ("long pair scaled to 200 kbp (same construction and rates as the 1 Mbp pair), "
+                "for profiling")
+    elif name == "small":
+        a, b, sc = synth.plain_small()
+        desc = "plain pair: 2,000 bp vs 400 + mutated 1,200 bp window + 400; scoring 1/-3/-5/-2"
+    else:
+        a, b, sc = synth.chromosome_pair()
+        desc = "chromosome pair: two ~10 Mbp from an 8 Mbp ancestor (3% sub, 0.5% indel) + 1 Mbp flanks"
+    return a, b, sc, desc
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = max(mx, float(f[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def profile_traffic(workload_name):
+    """DRAM bytes per stage-1 launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"stage1_{workload_name}_pair.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_baseline(a: bytes, b: bytes, sc):
+    """The oracle's multithreaded CPU wavefront (same int32 recurrence) on a
+    bounded sample of the same pair: a band of rows against all columns, sized
+    for about 12 s on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_ctypes as O
+    rows, cols, _ = O.orient(a, b)
+    threads = os.cpu_count() or 1
+    lo = len(rows) // 10
+    probe_rows = max(1, min(len(rows) - lo, int(2e9 // len(cols))))
+    _, t = O.stage1_mt(rows[lo:lo + probe_rows], cols, O.scoring(*sc), threads=threads)
+    rate = probe_rows * len(cols) / max(t, 1e-6)
+    nrows = max(1, min(len(rows) - lo, int(rate * 12.0 // len(cols))))
+    _, t = O.stage1_mt(rows[lo:lo + nrows], cols, O.scoring(*sc), threads=threads)
+    cells = nrows * len(cols)
+    return {"value": cells / t / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port",
+            "sample": f"rows {lo}..{lo + nrows} of the rows sequence x all {len(cols)} columns "
+                      f"({cells:.3e} cells, {t:.1f} s), score + end cell"}
+
+
+def reference_arm(args):
+    """The reference's own kernels, compiled for the CPU (oracle/_ref, host threads
+    standing in for its 2 x 5 CUDA threads), stage 1 on a bounded sample."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    a, b, sc, desc = workload(args.workload)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_ctypes as O
+    if not os.path.exists(O.REFEMU_PATH):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/swalign_emu was not built"}))
+        return
+    rows, cols, _ = O.orient(a, b)
+    lo = len(rows) // 10
+    na = min(len(rows) - lo, 6000)
+    nb = min(len(cols) - lo if len(cols) > lo + 100 else len(cols), 6000)
+    sa = rows[lo:lo + na]
+    sb = cols[lo:lo + nb] if len(cols) > lo + nb else cols[:nb]
+    td = tempfile.mkdtemp()
+    fa, fb = os.path.join(td, "a.fa"), os.path.join(td, "b.fa")
+    open(fa, "wb").write(b">sample a\n" + sa + b"\n")
+    open(fb, "wb").write(b">sample b\n" + sb + b"\n")
+    for _ in range(args.warmup):
+        O.run_reference(fa, fb, *sc, stage1_only=True)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.run_reference(fa, fb, *sc, stage1_only=True)
+    dt = time.perf_counter() - t0
+    cells = len(sa) * len(sb) * args.steps
+    v = cells / dt / 1e9
+    cores = 5  # one block of the reference's forced 2 x 5 runs at a time, one host thread per CUDA thread
+    line = {"metric": METRIC, "value": v, "unit": "GCUPS", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": desc, "sample_rows": len(sa), "sample_cols": len(sb),
+                       "stages": "stage 1 (score + end cell)"},
+            "cpu_baseline": {"value": v, "unit": "GCUPS", "cores": cores, "kind": "reference",
+                             "sample": f"{len(sa)} x {len(sb)} sub-pair of the workload, stage 1, "
+                                       f"reference kernels on host threads"},
+            "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import swb200
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    a, b, sc_t, desc = workload(args.workload)
+    sc = swb200.scoring(*sc_t)
+    m, n = max(len(a), len(b)), min(len(a), len(b))
+    rows_b, cols_b = (a, b) if len(a) >= len(b) else (b, a)
+    cells = m * n
+    stream = torch.cuda.current_stream()
+    ctx = swb200.Context(device=local, cuda_stream=stream.cuda_stream)
+    flags = swb200.FLAG_SCORE_ONLY if args.score_only else 0
+
+    d_rows = torch.frombuffer(bytearray(rows_b), dtype=torch.uint8).cuda()
+    d_cols = torch.frombuffer(bytearray(cols_b), dtype=torch.uint8).cuda()
+    h_a = torch.frombuffer(bytearray(a), dtype=torch.uint8).pin_memory()
+    h_b = torch.frombuffer(bytearray(b), dtype=torch.uint8).pin_memory()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step_device():
+        flush.zero_()
+        return ctx.align_device(d_rows.data_ptr(), m, d_cols.data_ptr(), n, sc, flags)
+
+    def step_host():
+        flush.zero_()
+        return ctx.align_ptr(h_a.data_ptr(), len(a), h_b.data_ptr(), len(b), sc, flags)
+
+    first = None
+    for _ in range(args.warmup):
+        first = step_device()
+    torch.cuda.synchronize()
+
+    def timed(fn):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        res = []
+        e0.record(stream)
+        for _ in range(args.steps):
+            res.append(fn())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        return ms, res
+
+    with ClockSampler(local) as clk:
+        ms_dev, res_dev = timed(step_device)
+    ms_e2e, res_e2e = timed(step_host)
+
+    for r in res_dev + res_e2e:
+        assert (r.score, r.end_row, r.end_col) == (first.score, first.end_row, first.end_col)
+
+    value = world * cells * args.steps / (ms_dev * 1e-3) / 1e9
+    e2e = world * cells * args.steps / (ms_e2e * 1e-3) / 1e9
+    k_ms = sum(r.stage1_ms for r in res_dev) / len(res_dev)
+    achieved = cells / (k_ms * 1e-3) / 1e9
+    peak_cells = swb200.probe_cell_peak(local)
+    peak = peak_cells["cells_per_s"] / 1e9
+    traffic = profile_traffic(args.workload)
+    launches = sum(r.kernel_launches for r in res_dev)
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    cpu = None if args.no_cpu_baseline else cpu_baseline(a, b, sc_t)
+    d2h = 64 + first.n_ops + 24 * len(first.xpoints)
+    line = {
+        "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_dev / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": desc, "rows": m, "cols": n, "score": first.score,
+                   "end": [first.end_row + 1, first.end_col + 1],
+                   "stages": "stage 1 only" if args.score_only else
+                             "stage 1 + special rows + GPU traceback (alignment, crosspoints)",
+                   "special_interval": first.special_interval,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "256 MiB buffer written before every step (inside the timed region)"},
+        "roofline": {"bound": "int32_dpx", "achieved": achieved, "peak": peak, "unit": "GCUPS",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": "stage1_kernel (scoring wavefront)",
+                     "peak_source": "measured: swb_probe_cell_peak (per-cell DPX/INT32 mix, full occupancy)",
+                     "stage1_ms": k_ms, "stage2_ms": sum(r.stage2_ms for r in res_dev) / len(res_dev)},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e, "unit": "GCUPS", "h2d_bytes_per_step": len(a) + len(b),
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

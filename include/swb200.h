@@ -89,6 +89,7 @@ typedef struct {
     int32_t     xpoint_interval;    /* rows between reference special rows (4*T)    */
     int32_t     special_interval;   /* rows between this run's HBM special rows     */
     int64_t     special_bytes;      /* HBM held by special rows for this call       */
+    int32_t     kernel_launches;    /* this library's kernels launched by the call  */
 } swb_result;
 
 typedef struct {
@@ -96,6 +97,8 @@ typedef struct {
     uint64_t hbm_budget_bytes;      /* cap on special rows + sequences; 0 = 40 GiB  */
     int32_t  special_interval;      /* special-row spacing in rows; 0 = autotune    */
     int32_t  verbose;               /* nonzero: progress lines on stderr             */
+    uint64_t cuda_stream;           /* a cudaStream_t of the caller to run on, cast
+                                       to an integer; 0 = the context's own stream */
 } swb_options;
 
 typedef struct swb_ctx swb_ctx;
@@ -137,6 +140,12 @@ void swb_result_free(swb_result *res);
  * when the reference could not launch (cols < 4). */
 int swb_reference_geometry(int64_t rows, int64_t cols, int32_t *G, int32_t *T, int64_t *P1,
                            int64_t *P2);
+
+/* Copies special row `idx` of the context's last call (row (idx+1)*interval - 1)
+ * as (H, F) int32 pairs into host memory out[2*cols]; *interval receives the
+ * spacing.  The reference keeps these rows in temp/row_<R> files
+ * (src/Builders.cpp:41-61, read back at src/Crosspointer.cpp:94-102). */
+int swb_special_row_copy(swb_ctx *ctx, int64_t idx, int32_t *out, int64_t cols, int64_t *interval);
 
 /* Library version string. */
 const char *swb_version(void);

@@ -49,7 +49,8 @@ int orc_stage1(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
                const orc_scoring *sc, int semantics, int tie, orc_end *out);
 
 /* Stage 1 on all `threads` host threads (blocked wavefront), textbook semantics.
- * Same result as orc_stage1(..., ORC_TEXTBOOK, tie, ...).  Returns elapsed ns in
+ * Same result as orc_stage1(..., ORC_TEXTBOOK, tie, ...); also accepts m < n
+ * (bands of rows used as timing samples).  Returns elapsed ns in
  * *ns_out when it is not NULL. */
 int orc_stage1_mt(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
                   const orc_scoring *sc, int tie, int threads, orc_end *out, int64_t *ns_out);

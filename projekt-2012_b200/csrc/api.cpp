@@ -50,6 +50,7 @@ struct swb_ctx {
     int device = 0;
     swb_options opts{};
     cudaStream_t stream = nullptr;
+    bool own_stream = true;
     int sms = 0;
     std::string err;
     DevBuf rows, cols, hbuf, progress, wbest, best, errf, srows, scols, work;
@@ -107,6 +108,7 @@ void swb_options_default(swb_options *o) {
     o->hbm_budget_bytes = 0;
     o->special_interval = 0;
     o->verbose = 0;
+    o->cuda_stream = 0;
 }
 
 int swb_ctx_create(const swb_options *opts, swb_ctx **out) {
@@ -131,11 +133,16 @@ int swb_ctx_create(const swb_options *opts, swb_ctx **out) {
     }
     if ((e = cudaSetDevice(c->device)) != cudaSuccess ||
         (e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device)) != cudaSuccess ||
-        (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (c->opts.cuda_stream == 0 &&
+         (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) ||
         (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess) {
         int rc = cuda_fail(nullptr, e, "swb_ctx_create");
         delete c;
         return rc;
+    }
+    if (c->opts.cuda_stream != 0) {
+        c->stream = (cudaStream_t)(uintptr_t)c->opts.cuda_stream;
+        c->own_stream = false;
     }
     *out = c;
     return SWB_OK;
@@ -150,7 +157,7 @@ void swb_ctx_destroy(swb_ctx *c) {
         b->release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
 }
 
@@ -317,6 +324,7 @@ int align_device(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_
     int rc = run_stage1(c, d_rows, m, d_cols, n, sc, flags, sr_interval, &best, &ms, &nsr);
     if (rc != SWB_OK) return rc;
     out->stage1_ms = ms;
+    out->kernel_launches += 2;  // stage-1 wavefront + best-cell reduction
     out->special_interval = (int32_t)c->last_sr_interval;
     out->special_bytes = (int64_t)sizeof(int2) * nsr * n;
     if (best.valid) {

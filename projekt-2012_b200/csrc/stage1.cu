@@ -39,7 +39,7 @@ namespace {
 constexpr int kCH = 8;         // columns per ring refill
 constexpr int kP = 16;         // refill lead: columns [k + kP, k + kP + kCH) at step k
 constexpr int kRing = 32;      // ring entries per warp (power of two >= kP + kCH)
-constexpr long long kSpinLimit = 1LL << 27;  // bounded waits (x ~1 us)
+constexpr unsigned long long kWaitLimitNs = 20ULL * 1000 * 1000 * 1000;  // bound of every wait
 
 enum : int32_t { kErrNone = 0, kErrTimeout = 4 };
 
@@ -50,6 +50,11 @@ __device__ __forceinline__ int32_t ld_acquire(const int32_t *p) {
     int32_t v;
     asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
 __device__ __forceinline__ int32_t ld_volatile(const int32_t *p) {
     return *reinterpret_cast<const volatile int32_t *>(p);
@@ -163,10 +168,10 @@ __device__ __forceinline__ bool refill(const Stage1Args &a, int4 *ring, int lane
     bool ok = true;
     if (lane < kCH) {
         const int64_t c = c0 + lane;
-        if (strip > 0) {
-            long long it = 0;
+        if (strip > 0 && ld_acquire(&a.progress[strip - 1]) < (int32_t)c1) {
+            const unsigned long long t0 = global_ns();
             while (ld_acquire(&a.progress[strip - 1]) < (int32_t)c1) {
-                if (++it > kSpinLimit || ld_volatile(&a.err[1]) != 0) {
+                if (ld_volatile(&a.err[1]) != 0 || global_ns() - t0 > kWaitLimitNs) {
                     ok = false;
                     break;
                 }

@@ -49,12 +49,13 @@ class Result(C.Structure):
                 ("n_ops", C.c_int64), ("ops", C.c_void_p),
                 ("n_xpoints", C.c_int64), ("xpoints", C.POINTER(XPoint)),
                 ("xpoint_interval", C.c_int32), ("special_interval", C.c_int32),
-                ("special_bytes", C.c_int64)]
+                ("special_bytes", C.c_int64), ("kernel_launches", C.c_int32)]
 
 
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64),
-                ("special_interval", C.c_int32), ("verbose", C.c_int32)]
+                ("special_interval", C.c_int32), ("verbose", C.c_int32),
+                ("cuda_stream", C.c_uint64)]
 
 
 class SwbError(RuntimeError):
@@ -97,6 +98,8 @@ def lib():
                                            C.POINTER(C.c_int64)]
         L.swb_special_row_copy.restype = C.c_int
         L.swb_version.restype = C.c_char_p
+        L.swb_probe_cell_peak.argtypes = [C.c_int32] + [C.POINTER(C.c_double)] * 5
+        L.swb_probe_cell_peak.restype = C.c_int
         _lib = L
     return _lib
 
@@ -123,6 +126,8 @@ class Alignment:
     xpoint_interval: int = 0
     special_interval: int = 0
     special_bytes: int = 0
+    kernel_launches: int = 0
+    n_ops: int = 0
 
 
 def _convert(r: Result) -> Alignment:
@@ -131,19 +136,22 @@ def _convert(r: Result) -> Alignment:
            for i in range(r.n_xpoints)]
     return Alignment(r.score, r.end_row, r.end_col, r.start_row, r.start_col, bool(r.swapped),
                      r.rows, r.cols, r.stage1_ms, r.stage2_ms, r.total_ms, ops, xps,
-                     r.xpoint_interval, r.special_interval, r.special_bytes)
+                     r.xpoint_interval, r.special_interval, r.special_bytes, r.kernel_launches,
+                     r.n_ops)
 
 
 class Context:
     """One device context (owns a CUDA stream and reusable device buffers)."""
 
-    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, special_interval: int = 0):
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, special_interval: int = 0,
+                 cuda_stream: int = 0):
         L = lib()
         o = Options()
         L.swb_options_default(C.byref(o))
         o.device = device
         o.hbm_budget_bytes = hbm_budget_bytes
         o.special_interval = special_interval
+        o.cuda_stream = cuda_stream
         h = C.c_void_p()
         rc = L.swb_ctx_create(C.byref(o), C.byref(h))
         if rc != SWB_OK:
@@ -173,6 +181,19 @@ class Context:
     def align(self, a: bytes, b: bytes, sc: Scoring, flags: int = 0) -> Alignment:
         r = Result()
         rc = lib().swb_align_pair(self._h, a, len(a), b, len(b), C.byref(sc), flags, C.byref(r))
+        if rc != SWB_OK:
+            self._err(rc)
+        try:
+            return _convert(r)
+        finally:
+            lib().swb_result_free(C.byref(r))
+
+    def align_ptr(self, p_a: int, la: int, p_b: int, lb: int, sc: Scoring, flags: int = 0) -> Alignment:
+        """Host sequences given by address (e.g. pinned buffers)."""
+        r = Result()
+        fn = lib().swb_align_pair
+        rc = fn(self._h, C.cast(C.c_void_p(p_a), C.c_char_p), la, C.cast(C.c_void_p(p_b), C.c_char_p), lb,
+                C.byref(sc), flags, C.byref(r))
         if rc != SWB_OK:
             self._err(rc)
         try:
@@ -211,3 +232,14 @@ def reference_geometry(rows: int, cols: int):
 
 def version() -> str:
     return lib().swb_version().decode()
+
+
+def probe_cell_peak(device: int = 0) -> dict:
+    """Measured peak cell-update rate of the stage-1 per-cell instruction mix
+    (swb_probe_cell_peak) and single-op rates."""
+    v = [C.c_double() for _ in range(5)]
+    rc = lib().swb_probe_cell_peak(device, *[C.byref(x) for x in v])
+    if rc != SWB_OK:
+        raise SwbError(rc, "probe failed")
+    return {"cells_per_s": v[0].value, "iadd_per_s": v[1].value, "viaddmax_per_s": v[2].value,
+            "vimax3_per_s": v[3].value, "probe_ms": v[4].value}

@@ -92,8 +92,10 @@ def test_medium_similar_pairs(gpu_ctx):
 def test_empty_inputs(gpu_ctx):
     r = gpu_ctx.align(b"", b"ACGT", swb200.scoring(1, -3, -5, -2), swb200.FLAG_SCORE_ONLY)
     assert (r.score, r.end_row, r.end_col) == (0, 0, 0)
-    r = gpu_ctx.align(b"ACGT", b"TTTT", swb200.scoring(1, -3, -5, -2), swb200.FLAG_SCORE_ONLY)
+    r = gpu_ctx.align(b"ACGA", b"TTTT", swb200.scoring(1, -3, -5, -2), swb200.FLAG_SCORE_ONLY)
     assert (r.score, r.end_row, r.end_col) == (0, 0, 0)
+    r = gpu_ctx.align(b"ACGT", b"TTTT", swb200.scoring(1, -3, -5, -2), swb200.FLAG_SCORE_ONLY)
+    assert (r.score, r.end_row, r.end_col) == (1, 3, 0)
 
 
 def test_device_pointer_path_matches_host_path(gpu_ctx):
