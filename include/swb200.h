@@ -147,6 +147,30 @@ int swb_reference_geometry(int64_t rows, int64_t cols, int32_t *G, int32_t *T, i
  * (src/Builders.cpp:41-61, read back at src/Crosspointer.cpp:94-102). */
 int swb_special_row_copy(swb_ctx *ctx, int64_t idx, int32_t *out, int64_t cols, int64_t *interval);
 
+/* Score and end cell of one pair, for callers that cannot allocate device
+ * memory.  No counterpart in the reference (its stage 1 allocates its buffers
+ * with cudaMalloc, src/SWutils.cpp:144-168).  Callers inside another framework's
+ * memory pool, under a no-allocation policy, or that must not fail on device
+ * memory pass the sequences (device memory of `device`, rows >= cols) and a host
+ * result; the kernel's scratch is a fixed array inside this library (about
+ * 16.4 MiB per device that loads it, held until exit).  Limits: cols <=
+ * SWB_NOALLOC_MAX_COLS, rows <= SWB_NOALLOC_MAX_ROWS, else SWB_EUNSUPPORTED.
+ * The first call on a device looks up the array's device address; make it
+ * before any stream capture.  Calls on one device that overlap on the GPU race
+ * on the shared array.  `cuda_stream` is a cudaStream_t cast to an integer
+ * (0 = legacy default stream); the call returns after the result is on the host.
+ * Score-only (no traceback).  Error text: swb_noalloc_last_error(). */
+#define SWB_NOALLOC_MAX_COLS (1 << 20)
+#define SWB_NOALLOC_MAX_ROWS (1 << 25)
+typedef struct {
+    int32_t score;
+    int64_t end_row, end_col;
+} swb_score;
+int swb_score_pair_noalloc(int32_t device, const void *d_rows, int64_t rows, const void *d_cols,
+                           int64_t cols, const swb_scoring *sc, uint32_t flags, uint64_t cuda_stream,
+                           swb_score *out);
+const char *swb_noalloc_last_error(void);
+
 /* Library version string. */
 const char *swb_version(void);
 
