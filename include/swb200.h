@@ -153,7 +153,7 @@ int swb_special_row_copy(swb_ctx *ctx, int64_t idx, int32_t *out, int64_t cols, 
  * memory pool, under a no-allocation policy, or that must not fail on device
  * memory pass the sequences (device memory of `device`, rows >= cols) and a host
  * result; the kernel's scratch is a fixed array inside this library (about
- * 16.4 MiB per device that loads it, held until exit).  Limits: cols <=
+ * 16.1 MiB per device that loads it, held until exit).  Limits: cols <=
  * SWB_NOALLOC_MAX_COLS, rows <= SWB_NOALLOC_MAX_ROWS, else SWB_EUNSUPPORTED.
  * The first call on a device looks up the array's device address; make it
  * before any stream capture.  Calls on one device that overlap on the GPU race

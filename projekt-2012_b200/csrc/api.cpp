@@ -224,12 +224,11 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
                const swb_scoring *sc, uint32_t flags, int64_t sr_interval_rows, swb::BestRec *best_out,
                float *ms_out, int64_t *nsr_out) {
     using namespace swb;
-    const int R = 16;
+    const int R = 32;
     Stage1Plan plan = stage1_plan(m, n, c->sms, R);
     const int64_t W = (int64_t)plan.blocks * plan.warps_per_block;
     cudaError_t e;
-    if ((e = c->hbuf.ensure(sizeof(int2) * (size_t)std::max<int64_t>(n, 1))) != cudaSuccess ||
-        (e = c->progress.ensure(sizeof(int32_t) * (size_t)plan.nstrips)) != cudaSuccess ||
+    if ((e = c->hbuf.ensure(sizeof(int4) * (size_t)std::max<int64_t>(n, 1))) != cudaSuccess ||
         (e = c->wbest.ensure(sizeof(BestRec) * (size_t)W)) != cudaSuccess ||
         (e = c->best.ensure(sizeof(BestRec))) != cudaSuccess ||
         (e = c->errf.ensure(2 * sizeof(int32_t))) != cudaSuccess)
@@ -245,8 +244,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     a.gx = std::max(sc->gap_open, sc->gap_extend);
     a.mt1 = sc->match - sc->gap_open;
     a.mm1 = sc->mismatch - sc->gap_open;
-    a.hbuf = (int2 *)c->hbuf.p;
-    a.progress = (int32_t *)c->progress.p;
+    a.hbuf = (int4 *)c->hbuf.p;
     a.nstrips = plan.nstrips;
     a.wbest = (BestRec *)c->wbest.p;
     a.best = (BestRec *)c->best.p;
@@ -280,7 +278,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     a.tie.T = T;
     a.tie.C = refok ? P2 / G : 1;
 
-    if ((e = cudaMemsetAsync(a.progress, 0, sizeof(int32_t) * (size_t)plan.nstrips, c->stream)) != cudaSuccess ||
+    if ((e = cudaMemsetAsync(a.hbuf, 0xFF, sizeof(int4) * (size_t)n, c->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(a.err, 0, 2 * sizeof(int32_t), c->stream)) != cudaSuccess)
         return cuda_fail(c, e, "stage 1 reset");
     cudaEventRecord(c->ev0, c->stream);

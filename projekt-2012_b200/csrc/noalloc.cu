@@ -7,7 +7,7 @@
 // on memory.  swb_score_pair_noalloc() serves them: the caller passes the two
 // sequences (device memory) and a host result struct, and every piece of
 // scratch the stage-1 kernel needs lives in one file-scope device array,
-// g_noalloc_scratch, of fixed size (kNoAllocScratchBytes, about 16.4 MiB), which
+// g_noalloc_scratch, of fixed size (kNoAllocScratchBytes, about 16.1 MiB), which
 // every GPU that loads this library holds until the process exits.
 //
 // The array's name is only a host-side stand-in in host code; the device address
@@ -15,7 +15,7 @@
 // current) on the first call on the device, and handed to the kernel.  That
 // first call therefore does the set-up and should come before any stream
 // capture.  All calls share the one array, which keeps the last call's contents:
-// the progress counters and error flags are cleared at the start of every call.
+// the row buffer's tags and the error flags are reset at the start of every call.
 // Each device has its own copy of the array, so calls on different devices are
 // independent; calls on the same device that overlap on the GPU (from two
 // streams or two host threads) race on it and must be serialised by the caller.
@@ -30,14 +30,11 @@ namespace {
 
 constexpr int64_t kMaxCols = SWB_NOALLOC_MAX_COLS;
 constexpr int64_t kMaxRows = SWB_NOALLOC_MAX_ROWS;
-constexpr int64_t kMinStripRows = 32 * 16;                         // smallest strip height used
-constexpr int64_t kMaxStrips = (kMaxRows + kMinStripRows - 1) / kMinStripRows;
 constexpr int64_t kMaxWarps = 4096;
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr size_t kOffHbuf = 0;
-constexpr size_t kOffProgress = kOffHbuf + align256(sizeof(int4) * (size_t)kMaxCols);
-constexpr size_t kOffWbest = kOffProgress + align256(sizeof(int32_t) * (size_t)kMaxStrips);
+constexpr size_t kOffWbest = kOffHbuf + align256(sizeof(int4) * (size_t)kMaxCols);
 constexpr size_t kOffBest = kOffWbest + align256(sizeof(BestRec) * (size_t)kMaxWarps);
 constexpr size_t kOffErr = kOffBest + align256(sizeof(BestRec));
 constexpr size_t kNoAllocScratchBytes = kOffErr + align256(2 * sizeof(int32_t));
@@ -107,8 +104,7 @@ extern "C" int swb_score_pair_noalloc(int32_t device, const void *d_rows, int64_
     int sms = 0;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
         return noalloc_fail(SWB_ECUDA, cudaGetErrorString(e));
-    Stage1Plan plan = stage1_plan(rows, cols, sms, 16);
-    if (plan.nstrips > kMaxStrips) return noalloc_fail(SWB_EUNSUPPORTED, "too many strips for the fixed scratch");
+    Stage1Plan plan = stage1_plan(rows, cols, sms, 32);
     if ((int64_t)plan.blocks * plan.warps_per_block > kMaxWarps) plan.blocks = (int)(kMaxWarps / plan.warps_per_block);
 
     Stage1Args a{};
@@ -121,8 +117,7 @@ extern "C" int swb_score_pair_noalloc(int32_t device, const void *d_rows, int64_
     a.gx = std::max(sc->gap_open, sc->gap_extend);
     a.mt1 = sc->match - sc->gap_open;
     a.mm1 = sc->mismatch - sc->gap_open;
-    a.hbuf = (int2 *)(base + kOffHbuf);
-    a.progress = (int32_t *)(base + kOffProgress);
+    a.hbuf = (int4 *)(base + kOffHbuf);
     a.wbest = (BestRec *)(base + kOffWbest);
     a.best = (BestRec *)(base + kOffBest);
     a.err = (int32_t *)(base + kOffErr);
@@ -141,7 +136,7 @@ extern "C" int swb_score_pair_noalloc(int32_t device, const void *d_rows, int64_
     cudaStream_t st = (cudaStream_t)(uintptr_t)cuda_stream;
     BestRec best{};
     int32_t errh[2] = {0, 0};
-    if ((e = cudaMemsetAsync(a.progress, 0, sizeof(int32_t) * (size_t)plan.nstrips, st)) != cudaSuccess ||
+    if ((e = cudaMemsetAsync(a.hbuf, 0xFF, sizeof(int4) * (size_t)cols, st)) != cudaSuccess ||
         (e = cudaMemsetAsync(a.err, 0, 2 * sizeof(int32_t), st)) != cudaSuccess ||
         (e = stage1_launch(a, plan, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(&best, a.best, sizeof best, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||

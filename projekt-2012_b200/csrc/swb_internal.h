@@ -34,18 +34,25 @@ struct TieGeom {
     int64_t C;     // reference column chunk P2 / G
 };
 
-// Device buffers and scalars for one stage-1 launch.
+// Device buffers and scalars for one stage-1 launch over a rectangle of the
+// matrix: rows [r_origin, r_origin + m) x cols [c_origin, c_origin + n).
 struct Stage1Args {
-    const uint8_t *rows;   // device, m bytes (longer sequence)
+    const uint8_t *rows;   // device, m bytes (the rectangle's rows)
     const uint8_t *cols;   // device, n bytes
     int64_t m, n;
     int32_t open, ext, gx; // gap_open, gap_extend, max(gap_open, gap_extend)
     int32_t mt1, mm1;      // match - open, mismatch - open
-    int2 *hbuf;            // n entries: (H + open, F of the next row) of the last strip bottom
-    int32_t *progress;     // nstrips entries, zeroed before the launch
+    int4 *hbuf;            // n entries {H + open, tag, F of the next row, tag}; 0xFF-filled per launch
     int2 *srows;           // special rows [nsr][n] of (H, F), or nullptr
     int64_t sr_every;      // a special row every sr_every strips
     int64_t nsr;           // number of special rows
+    int2 *scols;           // special columns [nsc][m] of (H, E), or nullptr
+    int32_t sc_every;      // a special column every sc_every columns (power of two)
+    int64_t nsc;
+    const int2 *top;       // (H, F) of the row above the rectangle, n entries, or nullptr (zero)
+    const int2 *left;      // (H, E) of the column left of the rectangle, m entries, or nullptr (zero)
+    int32_t corner;        // H above-left of the rectangle
+    int64_t r_origin, c_origin;  // rectangle origin in the whole matrix (tie key)
     int64_t nstrips;
     BestRec *wbest;        // one per warp of the grid
     BestRec *best;         // final reduced record
@@ -60,7 +67,7 @@ bool reference_geometry(int64_t rows, int64_t cols, int32_t *G, int32_t *T, int6
 
 // Stage-1 launch plan (chosen by the host for a pair).
 struct Stage1Plan {
-    int R = 16;            // rows per lane
+    int R = 32;            // rows per lane
     int warps_per_block = 4;
     int blocks = 0;
     int64_t strip_rows = 0;
