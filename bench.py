@@ -34,7 +34,8 @@ def parse_args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["long", "long200k", "small", "chromosome"], default="long")
+    p.add_argument("--workload", choices=["long", "long200k", "long1mx250k", "small", "chromosome"],
+                   default="long")
     p.add_argument("--score-only", action="store_true", help="stage 1 only (diagnostics)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -50,6 +51,11 @@ def workload(name):
         a, b, sc = synth.long_pair(length=200_000)
         desc = ("long pair scaled to 200 kbp (same construction and rates as the 1 Mbp pair), "
                 "for profiling")
+    elif name == "long1mx250k":
+        a, b, sc = synth.long_pair()
+        b = b[:250_000]
+        desc = ("the 1 Mbp long pair's rows against the first 250 kbp of its columns (same strip "
+                "count and occupancy as the full pair, a quarter of the steps), for profiling")
     elif name == "small":
         a, b, sc = synth.plain_small()
         desc = "plain pair: 2,000 bp vs 400 + mutated 1,200 bp window + 400; scoring 1/-3/-5/-2"

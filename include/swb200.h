@@ -96,7 +96,8 @@ typedef struct {
     int32_t  device;                /* CUDA device ordinal                           */
     uint64_t hbm_budget_bytes;      /* cap on special rows + sequences; 0 = 40 GiB  */
     int32_t  special_interval;      /* special-row spacing in rows; 0 = autotune    */
-    int32_t  verbose;               /* nonzero: progress lines on stderr             */
+    int32_t  verbose;               /* bit 0: progress lines on stderr; bit 1: record
+                                       the stage-1 strip trace (swb_trace_copy)     */
     uint64_t cuda_stream;           /* a cudaStream_t of the caller to run on, cast
                                        to an integer; 0 = the context's own stream */
 } swb_options;
@@ -170,6 +171,11 @@ int swb_score_pair_noalloc(int32_t device, const void *d_rows, int64_t rows, con
                            int64_t cols, const swb_scoring *sc, uint32_t flags, uint64_t cuda_stream,
                            swb_score *out);
 const char *swb_noalloc_last_error(void);
+
+/* Stage-1 strip trace of the context's last call when options.verbose has bit 1
+ * set: per strip {start ns, end ns, SM id} from %globaltimer / %smid, written to
+ * out[3*strips] (cap entries available); *count receives the strip count. */
+int swb_trace_copy(swb_ctx *ctx, int64_t *out, int64_t cap, int64_t *count);
 
 /* Library version string. */
 const char *swb_version(void);

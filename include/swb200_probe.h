@@ -20,6 +20,11 @@ extern "C" {
 int swb_probe_cell_peak(int32_t device, double *cells_per_s, double *iadd_per_s, double *viaddmax_per_s,
                         double *vimax3_per_s, double *elapsed_ms);
 
+/* Dependent-chain latency (SM cycles per operation, one thread) of up to six
+ * operations: IADD, max(x + a, b) written in C, __viaddmax_s32, __vimax3_s32,
+ * __viaddmax_s32_relu, max(x, b) written in C.  Returns 0 on success. */
+int swb_probe_latency(int32_t device, double *cycles_per_op, int32_t nops);
+
 #ifdef __cplusplus
 }
 #endif

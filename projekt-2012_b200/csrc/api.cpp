@@ -53,11 +53,13 @@ struct swb_ctx {
     bool own_stream = true;
     int sms = 0;
     std::string err;
-    DevBuf rows, cols, hbuf, progress, wbest, best, errf, srows, scols, work;
+    DevBuf rows, cols, hbuf, wbest, best, errf, srows, scols, work, flags, lut, rcode, ctab, trace;
+    int64_t last_nstrips = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::mutex mu;
     // last stage-1 special-row layout (for swb_special_row_copy)
     int64_t last_nsr = 0, last_n = 0, last_sr_interval = 0;
+    int32_t last_launches = 0;  // this library's kernels launched by the last stage 1
 };
 
 static int fail(swb_ctx *ctx, int code, const char *fmt, ...) {
@@ -152,8 +154,8 @@ void swb_ctx_destroy(swb_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (DevBuf *b : {&c->rows, &c->cols, &c->hbuf, &c->progress, &c->wbest, &c->best, &c->errf, &c->srows,
-                      &c->scols, &c->work})
+    for (DevBuf *b : {&c->rows, &c->cols, &c->hbuf, &c->wbest, &c->best, &c->errf, &c->srows, &c->scols,
+                      &c->work, &c->flags, &c->lut, &c->rcode, &c->ctab, &c->trace})
         b->release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -224,14 +226,34 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
                const swb_scoring *sc, uint32_t flags, int64_t sr_interval_rows, swb::BestRec *best_out,
                float *ms_out, int64_t *nsr_out) {
     using namespace swb;
-    const int R = 32;
-    Stage1Plan plan = stage1_plan(m, n, c->sms, R);
-    const int64_t W = (int64_t)plan.blocks * plan.warps_per_block;
+    int R = 16;
+    if (const char *rv = std::getenv("SWB_STAGE1_R")) R = std::atoi(rv);  // tuning override: 8, 16 or 32
     cudaError_t e;
+    // TAB mode when the column sequence has at most four distinct bytes and the
+    // shifted scores fit a signed byte
+    bool tab = false;
+    uint8_t lut[256];
+    c->last_launches = 2;  // wavefront + best-cell reduction
+    const int32_t mt1 = sc->match - sc->gap_open, mm1 = sc->mismatch - sc->gap_open;
+    if (mt1 >= -128 && mt1 <= 127 && mm1 >= -128 && mm1 <= 127 && !std::getenv("SWB_STAGE1_CMP")) {
+        uint32_t present[256];
+        if ((e = c->flags.ensure(256 * sizeof(uint32_t))) != cudaSuccess ||
+            (e = stage1_presence(d_cols, n, (uint32_t *)c->flags.p, c->stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(present, c->flags.p, sizeof present, cudaMemcpyDeviceToHost, c->stream)) !=
+                cudaSuccess ||
+            (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+            return cuda_fail(c, e, "column alphabet");
+        c->last_launches += 1;
+        int K = 0;
+        for (int i = 0; i < 256; ++i) lut[i] = present[i] ? (uint8_t)(K++) : 7;
+        tab = K <= 4;
+    }
+    Stage1Plan plan = stage1_plan(m, n, c->sms, R, tab);
+    const int64_t W = (int64_t)plan.blocks * plan.warps_per_block;
     if ((e = c->hbuf.ensure(sizeof(int4) * (size_t)std::max<int64_t>(n, 1))) != cudaSuccess ||
         (e = c->wbest.ensure(sizeof(BestRec) * (size_t)W)) != cudaSuccess ||
         (e = c->best.ensure(sizeof(BestRec))) != cudaSuccess ||
-        (e = c->errf.ensure(2 * sizeof(int32_t))) != cudaSuccess)
+        (e = c->errf.ensure(4 * sizeof(int32_t))) != cudaSuccess)
         return cuda_fail(c, e, "stage 1 buffers");
 
     Stage1Args a{};
@@ -242,8 +264,19 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     a.open = sc->gap_open;
     a.ext = sc->gap_extend;
     a.gx = std::max(sc->gap_open, sc->gap_extend);
-    a.mt1 = sc->match - sc->gap_open;
-    a.mm1 = sc->mismatch - sc->gap_open;
+    a.mt1 = mt1;
+    a.mm1 = mm1;
+    if (tab) {
+        if ((e = c->lut.ensure(256)) != cudaSuccess || (e = c->rcode.ensure((size_t)m + 64)) != cudaSuccess ||
+            (e = c->ctab.ensure(sizeof(uint32_t) * ((size_t)n + 64))) != cudaSuccess ||
+            (e = cudaMemcpyAsync(c->lut.p, lut, 256, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+            (e = stage1_encode(d_rows, m, d_cols, n, (const uint8_t *)c->lut.p, (uint8_t *)c->rcode.p,
+                               (uint32_t *)c->ctab.p, mt1, mm1, &a.tab_hi, c->stream)) != cudaSuccess)
+            return cuda_fail(c, e, "stage 1 encode");
+        c->last_launches += 1;
+        a.rcode = (const uint8_t *)c->rcode.p;
+        a.ctab = (const uint32_t *)c->ctab.p;
+    }
     a.hbuf = (int4 *)c->hbuf.p;
     a.nstrips = plan.nstrips;
     a.wbest = (BestRec *)c->wbest.p;
@@ -252,6 +285,13 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     a.srows = nullptr;
     a.sr_every = 1;
     a.nsr = 0;
+    a.trace = nullptr;
+    c->last_nstrips = plan.nstrips;
+    if (c->opts.verbose & 2) {  // stage-1 strip trace, read back with swb_trace_copy
+        if ((e = c->trace.ensure(sizeof(int64_t) * 3 * (size_t)plan.nstrips)) != cudaSuccess)
+            return cuda_fail(c, e, "trace buffer");
+        a.trace = (int64_t *)c->trace.p;
+    }
     if (sr_interval_rows > 0) {
         const int64_t every = std::max<int64_t>(1, sr_interval_rows / plan.strip_rows);
         const int64_t nsr = (m / plan.strip_rows) / every;
@@ -279,7 +319,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     a.tie.C = refok ? P2 / G : 1;
 
     if ((e = cudaMemsetAsync(a.hbuf, 0xFF, sizeof(int4) * (size_t)n, c->stream)) != cudaSuccess ||
-        (e = cudaMemsetAsync(a.err, 0, 2 * sizeof(int32_t), c->stream)) != cudaSuccess)
+        (e = cudaMemsetAsync(a.err, 0, 4 * sizeof(int32_t), c->stream)) != cudaSuccess)
         return cuda_fail(c, e, "stage 1 reset");
     cudaEventRecord(c->ev0, c->stream);
     if ((e = stage1_launch(a, plan, c->stream)) != cudaSuccess) return cuda_fail(c, e, "stage 1 launch");
@@ -322,7 +362,7 @@ int align_device(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_
     int rc = run_stage1(c, d_rows, m, d_cols, n, sc, flags, sr_interval, &best, &ms, &nsr);
     if (rc != SWB_OK) return rc;
     out->stage1_ms = ms;
-    out->kernel_launches += 2;  // stage-1 wavefront + best-cell reduction
+    out->kernel_launches += c->last_launches;
     out->special_interval = (int32_t)c->last_sr_interval;
     out->special_bytes = (int64_t)sizeof(int2) * nsr * n;
     if (best.valid) {
@@ -400,4 +440,15 @@ extern "C" int swb_special_row_copy(swb_ctx *c, int64_t idx, int32_t *out, int64
                                cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(c, e, "special row copy");
     return SWB_OK;
+}
+
+// Copies the stage-1 strip trace of the last call (options.verbose bit 1 set):
+// per strip {start ns, end ns, SM id}.  Returns the number of strips in *count.
+extern "C" int swb_trace_copy(swb_ctx *c, int64_t *out, int64_t cap, int64_t *count) {
+    if (!c || !out || !count) return fail(c, SWB_EINVAL, "swb_trace_copy: bad arguments");
+    *count = c->last_nstrips;
+    if (!c->trace.p || cap < 3 * c->last_nstrips) return fail(c, SWB_EINVAL, "no trace or buffer too small");
+    cudaSetDevice(c->device);
+    cudaError_t e = cudaMemcpy(out, c->trace.p, sizeof(int64_t) * 3 * (size_t)c->last_nstrips, cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? SWB_OK : cuda_fail(c, e, "trace copy");
 }

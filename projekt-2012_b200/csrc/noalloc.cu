@@ -37,7 +37,7 @@ constexpr size_t kOffHbuf = 0;
 constexpr size_t kOffWbest = kOffHbuf + align256(sizeof(int4) * (size_t)kMaxCols);
 constexpr size_t kOffBest = kOffWbest + align256(sizeof(BestRec) * (size_t)kMaxWarps);
 constexpr size_t kOffErr = kOffBest + align256(sizeof(BestRec));
-constexpr size_t kNoAllocScratchBytes = kOffErr + align256(2 * sizeof(int32_t));
+constexpr size_t kNoAllocScratchBytes = kOffErr + align256(4 * sizeof(int32_t));
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -104,7 +104,7 @@ extern "C" int swb_score_pair_noalloc(int32_t device, const void *d_rows, int64_
     int sms = 0;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
         return noalloc_fail(SWB_ECUDA, cudaGetErrorString(e));
-    Stage1Plan plan = stage1_plan(rows, cols, sms, 32);
+    Stage1Plan plan = stage1_plan(rows, cols, sms, 16, false);
     if ((int64_t)plan.blocks * plan.warps_per_block > kMaxWarps) plan.blocks = (int)(kMaxWarps / plan.warps_per_block);
 
     Stage1Args a{};
@@ -137,7 +137,7 @@ extern "C" int swb_score_pair_noalloc(int32_t device, const void *d_rows, int64_
     BestRec best{};
     int32_t errh[2] = {0, 0};
     if ((e = cudaMemsetAsync(a.hbuf, 0xFF, sizeof(int4) * (size_t)cols, st)) != cudaSuccess ||
-        (e = cudaMemsetAsync(a.err, 0, 2 * sizeof(int32_t), st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(a.err, 0, 4 * sizeof(int32_t), st)) != cudaSuccess ||
         (e = stage1_launch(a, plan, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(&best, a.best, sizeof best, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(errh, a.err, sizeof errh, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||

@@ -74,8 +74,55 @@ __global__ void single_op_kernel(const int32_t *in, int32_t *out, int iters, int
     out[tid] = acc;
 }
 
+// Dependent-chain latency in SM cycles per operation, one thread.
+// op: 0 IADD, 1 max(x + a, b) in plain C, 2 __viaddmax_s32, 3 __vimax3_s32,
+//     4 __viaddmax_s32_relu, 5 max(x, b) in plain C
+__global__ void latency_kernel(const int32_t *in, int32_t *out, int iters, int op, long long *cycles) {
+    int32_t x = in[0];
+    const int32_t a = in[1], b = in[2];
+    const long long t0 = clock64();
+    switch (op) {
+        case 0: for (int i = 0; i < iters; ++i) x = x + a; break;
+        case 1: for (int i = 0; i < iters; ++i) x = max(x + a, b + i); break;
+        case 2: for (int i = 0; i < iters; ++i) x = __viaddmax_s32(x, a, b + i); break;
+        case 3: for (int i = 0; i < iters; ++i) x = __vimax3_s32(x, a + i, b); break;
+        case 4: for (int i = 0; i < iters; ++i) x = __viaddmax_s32_relu(x, a, b + i); break;
+        default: for (int i = 0; i < iters; ++i) x = max(x, b + i); break;
+    }
+    const long long t1 = clock64();
+    out[0] = x;
+    *cycles = t1 - t0;
+}
+
 }  // namespace
 }  // namespace swb
+
+extern "C" int swb_probe_latency(int32_t device, double *cycles_per_op, int32_t nops) {
+    using namespace swb;
+    if (cudaSetDevice(device) != cudaSuccess) return SWB_ECUDA;
+    int32_t hin[4] = {3, -2, -7, 0};
+    int32_t *din = nullptr, *dout = nullptr;
+    long long *dcyc = nullptr;
+    if (cudaMalloc(&din, sizeof hin) != cudaSuccess || cudaMalloc(&dout, 16) != cudaSuccess ||
+        cudaMalloc(&dcyc, sizeof(long long)) != cudaSuccess)
+        return SWB_ENOMEM;
+    cudaMemcpy(din, hin, sizeof hin, cudaMemcpyHostToDevice);
+    const int iters = 1 << 16;
+    for (int op = 0; op < nops && op < 6; ++op) {
+        long long best = -1;
+        for (int rep = 0; rep < 3; ++rep) {
+            latency_kernel<<<1, 1>>>(din, dout, iters, op, dcyc);
+            long long c = 0;
+            cudaMemcpy(&c, dcyc, sizeof c, cudaMemcpyDeviceToHost);
+            if (best < 0 || c < best) best = c;
+        }
+        cycles_per_op[op] = (double)best / iters;
+    }
+    cudaFree(din);
+    cudaFree(dout);
+    cudaFree(dcyc);
+    return cudaGetLastError() == cudaSuccess ? SWB_OK : SWB_ECUDA;
+}
 
 extern "C" int swb_probe_cell_peak(int32_t device, double *cells_per_s, double *iadd_per_s,
                                    double *viaddmax_per_s, double *vimax3_per_s, double *elapsed_ms) {

@@ -12,17 +12,21 @@
 //     row at the previous step is exactly the top boundary lane l needs now; it
 //     moves by one rotating warp shuffle per value.  Lane 31 turns its shuffle
 //     slot around: it sends lane 0 the next column's top boundary and column
-//     byte, read from a per-warp shared-memory ring.
+//     value, read from a per-warp shared-memory ring.
 //   * Strips are chained through one L2-resident row buffer `hbuf` of 16-byte
 //     entries {H + open, tag, F, tag}, written by the strip above with one
 //     vector store and read by the strip below with one vector load (each 8-byte
 //     half is a single access, so a matching tag in both halves proves the
 //     entry is complete; no fences or counters are needed).  The strip below
-//     issues its loads one refill ahead and checks the tags a refill later; a
-//     mismatch is re-polled with a bounded wait.
+//     issues its loads one refill (8 steps) ahead and checks the tags a refill
+//     later; a mismatch is re-polled with a bounded wait.
 //   * The grid is persistent and cooperative (every warp resident).  Strip s runs
 //     on block s mod B, warp (s / B) mod 4, so consecutive strips sit on
 //     different SMs and every SM gets the same number of strips (+-1).
+//   * Substitution score: with at most four distinct column bytes (DNA) a
+//     per-column table word holds (s - open) for codes 0..3 and one PRMT with a
+//     per-row selector picks the sign-extended score (TAB); otherwise the raw
+//     bytes are compared (CMP).
 //   * Optional outputs: special rows (H, F) every `sr_every` strips (the strip's
 //     bottom row) and special columns (H, E) every `sc_every` columns.
 //   * Optional inputs (traceback recompute of a sub-rectangle): the row above
@@ -35,6 +39,7 @@
 //     HO  = max(F + open, t + open)                           __viaddmax_s32
 //     F'  = max(F + max(ext, open), t + open)  (F of the row below)
 // which equals H = max(0, E, F, H_diag + s), F' = max(F + ext, H + open).
+#include <algorithm>
 #include <climits>
 
 #include "swb_internal.h"
@@ -43,19 +48,13 @@ namespace swb {
 
 namespace {
 
-constexpr int kCH = 8;         // columns per ring refill
-constexpr int kP = 8;          // ring entries for columns [k + kP, k + kP + kCH) are stored at step k
+constexpr int kCH = 8;         // steps per refill
 constexpr int kRing = 32;      // ring entries per warp
 constexpr int kWarps = 4;      // warps per block
-constexpr unsigned long long kWaitLimitNs = 20ULL * 1000 * 1000 * 1000;  // bound of every wait
+constexpr long long kWaitLimitCycles = 40LL * 1000 * 1000 * 1000;  // bound of every wait (~20 s)
 
 enum : int32_t { kErrNone = 0, kErrTimeout = 4 };
 
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
 __device__ __forceinline__ int32_t ld_volatile(const int32_t *p) {
     return *reinterpret_cast<const volatile int32_t *>(p);
 }
@@ -71,16 +70,25 @@ __device__ __forceinline__ void st_ll(int4 *p, int32_t ho, int32_t f, int32_t ta
     asm volatile("st.volatile.global.v4.s32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(ho), "r"(tag), "r"(f), "r"(tag)
                  : "memory");
 }
+// Byte permute with per-nibble sign replication (PTX prmt default mode).
+__device__ __forceinline__ int32_t prmt(uint32_t lo, uint32_t hi, uint32_t sel) {
+    int32_t r;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(lo), "r"(hi), "r"(sel));
+    return r;
+}
 
 __device__ __noinline__ uint64_t tie_key(const TieGeom g, int64_t r, int64_t c) {
     if (g.mode == kTieRowMajor) return ((uint64_t)r << 32) | (uint64_t)c;
-    const int64_t T = g.T, G = g.G, C = g.C;
-    const int64_t t = (r >> 2) % T;
-    const int64_t s = r / (4 * T);
-    const int64_t k = (c + t) / C;
-    const int64_t b = G - 1 - (k % G);
-    return ((uint64_t)(b * T + t) << 60) | ((uint64_t)(s + k) << 32) |
-           ((uint64_t)(c + t - k * C) << 2) | (uint64_t)(r & 3);
+    // rows and columns are below 2^31: 32-bit arithmetic
+    const uint32_t T = (uint32_t)g.T, G = (uint32_t)g.G, C = (uint32_t)g.C;
+    const uint32_t r32 = (uint32_t)r, c32 = (uint32_t)c;
+    const uint32_t q = r32 >> 2;
+    const uint32_t t = q % T;
+    const uint32_t s = q / T;
+    const uint32_t k = (c32 + t) / C;
+    const uint32_t b = G - 1 - (k % G);
+    return ((uint64_t)(b * T + t) << 60) | ((uint64_t)(s + k) << 32) | ((uint64_t)(c32 + t - k * C) << 2) |
+           (uint64_t)(r32 & 3);
 }
 
 __device__ __forceinline__ bool better(int32_t ho, uint64_t key, int32_t bho, uint64_t bkey) {
@@ -94,31 +102,39 @@ struct Best {
 };
 
 // Rows of `mask` hold the column maximum cm at column j: keep the smallest key.
-__device__ __forceinline__ void slow_best(uint32_t mask, int32_t cm, const Stage1Args &a, Best &b,
-                                          int64_t row0, int32_t j) {
+// Out of line, so the hot loop keeps only the threshold in a register.
+__device__ __noinline__ int32_t slow_best(uint32_t mask, int32_t cm, const TieGeom tie, int64_t m, int64_t r_origin,
+                                          int64_t c_origin, Best *b, int64_t row0, int32_t j, int32_t *gbest,
+                                          int32_t open) {
+    const int32_t before = b->ho;
     while (mask) {
         const int i = __ffs(mask) - 1;
         mask &= mask - 1;
         const int64_t r = row0 + i;
-        if (r >= a.m) break;
-        const uint64_t key = tie_key(a.tie, a.r_origin + r, (int64_t)a.c_origin + j);
-        if (better(cm, key, b.ho, b.key)) {
-            b.ho = cm;
-            b.key = key;
-            b.row = r;
-            b.col = j;
+        if (r >= m) break;
+        const uint64_t key = tie_key(tie, r_origin + r, c_origin + j);
+        if (better(cm, key, b->ho, b->key)) {
+            b->ho = cm;
+            b->key = key;
+            b->row = r;
+            b->col = j;
         }
     }
+    if (b->ho > before) atomicMax(gbest, b->ho - open);
+    return b->ho;
 }
 
 template <int R>
 struct Lane {
-    int32_t ra[R];   // row bytes (256 for rows past the end: never equal to a byte)
+    uint32_t ra[R];  // TAB: prmt selector of the row code; CMP: row byte (256 past the end)
     int32_t HO[R];   // H + open of the previous column
     int32_t E[R];    // E of the previous column
-    int32_t inHO, inF, inB;  // from the lane above: HO of its last row, F of my row 0, column byte
+    int32_t inHO, inF;       // from the lane above: HO of its last row, F of my row 0
+    uint32_t inB;            // column value: TAB table word / CMP byte
     int32_t hodPrev;         // HO of the row above my row 0 at the previous column
     int32_t hodInit;         // HO of the row above my row 0 left of column 0
+    int32_t bho;             // this lane's best HO (copy of best.ho)
+    int32_t thr;             // candidate threshold: max(bho, device-wide best H + open)
 };
 
 struct StripCtx {
@@ -130,18 +146,21 @@ struct StripCtx {
 };
 
 // One anti-diagonal step.  PRED: some lanes of the warp are outside [0, n).
-template <int R, bool PRED>
-__device__ __forceinline__ void step(Lane<R> &L, const Stage1Args &a, Best &b, const int4 *ring, int lane,
+// SC: this step may be a special-column step of some lane.
+template <int R, bool TAB, bool PRED, bool SC>
+__device__ __forceinline__ void step(Lane<R> &L, const Stage1Args &a, Best *b, const int4 *ring, int lane,
                                      const StripCtx &sc, int32_t k) {
     const int32_t j = k - lane;
     const bool act = !PRED || (j >= 0 && j < sc.n);
-    const int32_t cb = L.inB;
+    const uint32_t cb = L.inB;
     int32_t hod = (PRED && j == 0) ? L.hodInit : L.hodPrev;
     int32_t f = L.inF;
     int32_t flast = 0;
 #pragma unroll
     for (int i = 0; i < R; ++i) {
-        const int32_t s1 = (L.ra[i] == cb) ? a.mt1 : a.mm1;
+        int32_t s1;
+        if (TAB) s1 = prmt(cb, a.tab_hi, L.ra[i]);
+        else s1 = (L.ra[i] == cb) ? a.mt1 : a.mm1;
         const int32_t e = __viaddmax_s32(L.E[i], a.ext, L.HO[i]);
         const int32_t t = __viaddmax_s32_relu(hod, s1, e);
         const int32_t to = t + a.open;
@@ -158,14 +177,14 @@ __device__ __forceinline__ void step(Lane<R> &L, const Stage1Args &a, Best &b, c
 #pragma unroll
     for (int i = 1; i + 1 < R; i += 2) cm = __vimax3_s32(cm, L.HO[i], L.HO[i + 1]);
     if (R % 2 == 0) cm = max(cm, L.HO[R - 1]);
-    if (act && cm >= b.ho) {
+    if (act && cm >= L.thr) {
         uint32_t mask = 0;
 #pragma unroll
         for (int i = 0; i < R; ++i) mask |= (L.HO[i] == cm ? 1u : 0u) << i;
-        slow_best(mask, cm, a, b, sc.row0, j);
+        L.bho = slow_best(mask, cm, a.tie, a.m, a.r_origin, a.c_origin, b, sc.row0, j, a.err + 2, a.open);
+        L.thr = max(L.thr, L.bho);
     }
-    // special column: this lane's rows at column j
-    if (a.scols != nullptr && act && ((j + 1) & (a.sc_every - 1)) == 0) {
+    if (SC && act && ((j + 1) & (a.sc_every - 1)) == 0) {
         int2 *dst = a.scols + (int64_t)((j + 1) / a.sc_every - 1) * a.m + sc.row0;
 #pragma unroll
         for (int i = 0; i < R; ++i)
@@ -181,7 +200,7 @@ __device__ __forceinline__ void step(Lane<R> &L, const Stage1Args &a, Best &b, c
     }
     const int32_t oHO = last ? rv.x : L.HO[R - 1];
     const int32_t oF = last ? rv.y : f;
-    const int32_t oB = last ? rv.z : cb;
+    const uint32_t oB = last ? (uint32_t)rv.z : cb;
     L.hodPrev = L.inHO;
     const int src = (lane + 31) & 31;
     L.inHO = __shfl_sync(0xffffffffu, oHO, src);
@@ -189,64 +208,76 @@ __device__ __forceinline__ void step(Lane<R> &L, const Stage1Args &a, Best &b, c
     L.inB = __shfl_sync(0xffffffffu, oB, src);
 }
 
-// Top-boundary entry of column c for the first strip of the rectangle.
-__device__ __forceinline__ int4 top_entry(const Stage1Args &a, int32_t c) {
-    int4 v;
-    if (a.top) {
-        const int2 t = a.top[c];
-        v.x = t.x + a.open;
-        v.y = max(t.y + a.ext, t.x + a.open);
-    } else {
-        v.x = a.open;  // H = 0 above the first row
-        v.y = a.gx;    // F of row 0 = max(0 + ext, 0 + open)
-    }
-    v.z = (int32_t)a.cols[c];
-    v.w = 0;
-    return v;
+// Column value of column c: the table word (TAB) or the byte (CMP).
+template <bool TAB>
+__device__ __forceinline__ uint32_t col_value(const Stage1Args &a, int32_t c) {
+    if (TAB) return a.ctab[c];
+    return (uint32_t)a.cols[c];
 }
 
-// Ring refill at step k (k % kCH == 0): lanes 0..kCH-1 check the entries they
-// loaded one refill ago (columns [k+kP, k+kP+kCH)), store them in the ring and
-// issue the loads for the next refill.  Returns false on timeout/abort.
+// Prefetched inputs of one ring entry (held in registers for one refill).
+struct Pre {
+    int4 h;        // hbuf entry (strip > 0) or top boundary values (strip 0)
+    uint32_t cv;   // column value
+};
+
+template <bool TAB>
+__device__ __forceinline__ void prefetch(const Stage1Args &a, int32_t strip, int32_t c, Pre &p) {
+    p.cv = col_value<TAB>(a, c);
+    if (strip > 0) {
+        p.h = ld_ll(a.hbuf + c);
+    } else if (a.top) {
+        const int2 t = a.top[c];
+        p.h.x = t.x + a.open;
+        p.h.y = 0;
+        p.h.z = max(t.y + a.ext, t.x + a.open);
+        p.h.w = 0;
+    } else {
+        p.h.x = a.open;  // H = 0 above the first row
+        p.h.y = 0;
+        p.h.z = a.gx;    // F of row 0 = max(0 + ext, 0 + open)
+        p.h.w = 0;
+    }
+}
+
+// Stores the prefetched entry of column c into the ring (re-polling until the
+// strip above has written it).  Returns false on timeout/abort.
+__device__ __forceinline__ bool commit(const Stage1Args &a, int4 *ring, int32_t strip, int32_t c, Pre &p) {
+    if (strip > 0 && (p.h.y != strip - 1 || p.h.w != strip - 1)) {
+        const long long t0 = clock64();
+        for (;;) {
+            __nanosleep(32);
+            p.h = ld_ll(a.hbuf + c);
+            if (p.h.y == strip - 1 && p.h.w == strip - 1) break;
+            if (ld_volatile(&a.err[1]) != 0 || clock64() - t0 > kWaitLimitCycles) return false;
+        }
+    }
+    ring[c & (kRing - 1)] = make_int4(p.h.x, p.h.z, (int32_t)p.cv, 0);
+    return true;
+}
+
+// Refill at step k (k % kCH == 0): lanes 0..kCH-1 commit columns [k+kCH, k+2kCH)
+// (prefetched one refill ago) and prefetch columns [k+2kCH, k+3kCH).
+template <bool TAB>
 __device__ __forceinline__ bool refill(const Stage1Args &a, int4 *ring, int lane, int32_t strip, int32_t n,
-                                       int32_t k, int4 &pre) {
+                                       int32_t k, Pre &pre, int32_t &thr, int32_t bho) {
+    // cells below the best H found anywhere so far can never win: raise the
+    // candidate threshold to it (ties at that value are still examined)
+    thr = max(bho, ld_volatile(a.err + 2) + a.open);
     bool ok = true;
     if (lane < kCH) {
-        const int32_t c = k + kP + lane;
-        if (c < n) {
-            int4 v;
-            if (strip == 0) {
-                v = top_entry(a, c);
-            } else {
-                v = pre;
-                if (v.y != strip - 1 || v.w != strip - 1) {
-                    const unsigned long long t0 = global_ns();
-                    for (;;) {
-                        v = ld_ll(a.hbuf + c);
-                        if (v.y == strip - 1 && v.w == strip - 1) break;
-                        if (ld_volatile(&a.err[1]) != 0 || global_ns() - t0 > kWaitLimitNs) {
-                            ok = false;
-                            break;
-                        }
-                        __nanosleep(32);
-                    }
-                }
-                v.y = v.z;                        // F
-                v.z = (int32_t)a.cols[c];
-                v.w = 0;
-            }
-            ring[c & (kRing - 1)] = v;
-        }
+        const int32_t c = k + kCH + lane;
+        if (c < n) ok = commit(a, ring, strip, c, pre);
         const int32_t cn = c + kCH;
-        if (strip > 0 && cn < n) pre = ld_ll(a.hbuf + cn);
+        if (cn < n) prefetch<TAB>(a, strip, cn, pre);
     }
     const bool all_ok = __all_sync(0xffffffffu, ok);
     __syncwarp();
     return all_ok;
 }
 
-template <int R>
-__device__ __forceinline__ bool run_strip(const Stage1Args &a, int4 *ring, int lane, int32_t s, Best &b) {
+template <int R, bool TAB>
+__device__ bool run_strip(const Stage1Args &a, int4 *ring, int lane, int32_t s, Best *b, int32_t &bho) {
     Lane<R> L;
     StripCtx sc;
     const int64_t H = 32LL * R;
@@ -255,11 +286,19 @@ __device__ __forceinline__ bool run_strip(const Stage1Args &a, int4 *ring, int l
     sc.n = (int32_t)a.n;
     sc.sr = a.srows != nullptr && ((int64_t)(s + 1) % a.sr_every) == 0 && (int64_t)(s + 1) * H <= a.m;
     sc.sr_off = sc.sr ? ((int64_t)(s + 1) / a.sr_every - 1) * a.n : 0;
+    L.bho = bho;
+    L.thr = max(bho, ld_volatile(a.err + 2) + a.open);
 #pragma unroll
     for (int i = 0; i < R; ++i) {
         const int64_t r = sc.row0 + i;
         const bool in = r < a.m;
-        L.ra[i] = in ? (int32_t)a.rows[r] : 256;
+        if (TAB) {
+            const uint32_t q = in ? (uint32_t)a.rcode[r] : 7u;  // code 7 never matches
+            const uint32_t qs = q | 8u;
+            L.ra[i] = q | (qs << 4) | (qs << 8) | (qs << 12);
+        } else {
+            L.ra[i] = in ? (uint32_t)a.rows[r] : 256u;
+        }
         if (a.left && in) {
             const int2 lv = a.left[r];
             L.HO[i] = lv.x + a.open;
@@ -274,88 +313,96 @@ __device__ __forceinline__ bool run_strip(const Stage1Args &a, int4 *ring, int l
     else L.hodInit = a.open;
 
     const int32_t n = sc.n;
-    // prologue: ring entries for columns [0, kP + kCH), prefetch for the first refill
-    int4 pre = make_int4(0, 0, 0, 0);
+    // prologue: ring entries for columns [0, 2kCH); prefetch [2kCH, 3kCH)
+    Pre pre;
+    bool ok = true;
     if (lane < kCH) {
-        const int32_t c = kP + kCH + lane;
-        if (s > 0 && c < n) pre = ld_ll(a.hbuf + c);
-    }
-    for (int32_t c0 = 0; c0 < kP + kCH; c0 += kCH) {
-        bool ok = true;
-        if (lane < kCH && c0 + lane < n) {
-            const int32_t c = c0 + lane;
-            int4 v;
-            if (s == 0) {
-                v = top_entry(a, c);
-            } else {
-                const unsigned long long t0 = global_ns();
-                for (;;) {
-                    v = ld_ll(a.hbuf + c);
-                    if (v.y == s - 1 && v.w == s - 1) break;
-                    if (ld_volatile(&a.err[1]) != 0 || global_ns() - t0 > kWaitLimitNs) {
-                        ok = false;
-                        break;
-                    }
-                    __nanosleep(64);
-                }
-                v.y = v.z;
-                v.z = (int32_t)a.cols[c];
-                v.w = 0;
+        for (int32_t c = lane; c < 2 * kCH && ok; c += kCH) {
+            if (c < n) {
+                prefetch<TAB>(a, s, c, pre);
+                ok = commit(a, ring, s, c, pre);
             }
-            ring[c & (kRing - 1)] = v;
         }
-        if (!__all_sync(0xffffffffu, ok)) return false;
-        __syncwarp();
+        if (2 * kCH + lane < n) prefetch<TAB>(a, s, 2 * kCH + lane, pre);
+    }
+    if (!__all_sync(0xffffffffu, ok)) return false;
+    __syncwarp();
+    if (a.trace && lane == 0) {  // prologue done: the strip above has delivered columns [0, 2kCH)
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        a.trace[3 * s] = (int64_t)t;
     }
     {
         const int4 v = ring[0];
         L.inHO = v.x;
         L.inF = v.y;
-        L.inB = v.z;
+        L.inB = (uint32_t)v.z;
         L.hodPrev = L.hodInit;
     }
 
+    // Steps: [0, 32) ramp-up (predicated), [32, kB) steady, [kB, n + 31) ramp-down.
+    // Refills at every multiple of kCH except 0.  In the steady part, only the
+    // 32 steps after a multiple of sc_every hold special-column stores.
     const int32_t kEnd = n + 31;
     const int32_t kA = min(32, kEnd);
     int32_t kB = kA;
     if (n > 32) kB = 32 + ((n - 32) / kCH) * kCH;
     int32_t k = 0;
-    // the first refill is at k = 8 (columns [16, 24)); prologue covered [0, 16)
     for (; k < kA; ++k) {
-        if (k > 0 && (k % kCH) == 0 && !refill(a, ring, lane, s, n, k, pre)) return false;
-        step<R, true>(L, a, b, ring, lane, sc, k);
+        if (k > 0 && (k % kCH) == 0 && !refill<TAB>(a, ring, lane, s, n, k, pre, L.thr, L.bho)) return false;
+        if (a.scols) step<R, TAB, true, true>(L, a, b, ring, lane, sc, k);
+        else step<R, TAB, true, false>(L, a, b, ring, lane, sc, k);
     }
-    for (; k < kB; ++k) {
-        if ((k % kCH) == 0 && !refill(a, ring, lane, s, n, k, pre)) return false;
-        step<R, false>(L, a, b, ring, lane, sc, k);
+    while (k < kB) {
+        if (!refill<TAB>(a, ring, lane, s, n, k, pre, L.thr, L.bho)) return false;
+        // lane l stores special column j = q*sc_every - 1 at step j + l: a chunk of
+        // steps [k, k+kCH) needs the check when some (t + 1) mod sc_every < 32
+        const bool sc_window = a.scols != nullptr && ((k + kCH) & (a.sc_every - 1)) < 32 + kCH;
+        if (sc_window) {
+            for (int u = 0; u < kCH; ++u) step<R, TAB, false, true>(L, a, b, ring, lane, sc, k + u);
+        } else {
+            for (int u = 0; u < kCH; ++u) step<R, TAB, false, false>(L, a, b, ring, lane, sc, k + u);
+        }
+        k += kCH;
     }
     for (; k < kEnd; ++k) {
-        if ((k % kCH) == 0 && !refill(a, ring, lane, s, n, k, pre)) return false;
-        step<R, true>(L, a, b, ring, lane, sc, k);
+        if ((k % kCH) == 0 && !refill<TAB>(a, ring, lane, s, n, k, pre, L.thr, L.bho)) return false;
+        if (a.scols) step<R, TAB, true, true>(L, a, b, ring, lane, sc, k);
+        else step<R, TAB, true, false>(L, a, b, ring, lane, sc, k);
     }
+    bho = L.bho;
     return true;
 }
 
-template <int R>
-__global__ void __launch_bounds__(kWarps * 32) stage1_kernel(Stage1Args a) {
+template <int R, bool TAB>
+__global__ void __launch_bounds__(kWarps * 32, (R <= 16 ? 4 : 2)) stage1_kernel(Stage1Args a) {
     __shared__ int4 ring_all[kWarps][kRing];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     int4 *ring = ring_all[wib];
     const int64_t B = gridDim.x;
-    const int64_t per_round = B * kWarps;
 
     Best b;
     b.ho = a.open + 1;  // only H >= 1 is recorded
     b.key = ~0ULL;
     b.row = 0;
     b.col = 0;
+    int32_t bho = b.ho;
     bool failed = false;
     for (int64_t round = 0; !failed; ++round) {
         const int64_t s = blockIdx.x + B * (wib + kWarps * round);
         if (s >= a.nstrips) break;
-        (void)per_round;
-        if (!run_strip<R>(a, ring, lane, (int32_t)s, b)) failed = true;
+        if (a.trace && lane == 0) {
+            uint32_t smid;
+            asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+            a.trace[3 * s + 2] = (int64_t)smid;
+        }
+        if (!run_strip<R, TAB>(a, ring, lane, (int32_t)s, &b, bho)) failed = true;
+        if (a.trace && lane == 0) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            a.trace[3 * s + 1] = (int64_t)t;
+        }
     }
     if (failed && lane == 0) {
         atomicCAS(&a.err[0], kErrNone, kErrTimeout);
@@ -410,42 +457,67 @@ __global__ void reduce_best_kernel(const BestRec *in, int64_t count, BestRec *ou
     if (threadIdx.x == 0) *out = sh[0];
 }
 
-template <int R>
+// Row codes and column table words for TAB mode; lut maps a byte to its code
+// (0..3 for the column alphabet, 7 for every other byte).
+__global__ void encode_kernel(const uint8_t *rows, int64_t m, const uint8_t *cols, int64_t n, const uint8_t *lut,
+                              uint8_t *rcode, uint32_t *ctab, uint32_t mm4, uint32_t x1) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) rcode[i] = lut[rows[i]];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t q = lut[cols[i]];
+        ctab[i] = q < 4 ? (mm4 ^ (x1 << (8 * q))) : mm4;
+    }
+}
+
+// Byte presence flags of a sequence (for choosing TAB mode).
+__global__ void presence_kernel(const uint8_t *seq, int64_t n, uint32_t *flags) {
+    __shared__ uint32_t sh[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) sh[seq[i]] = 1;
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+        if (sh[i]) flags[i] = 1;
+}
+
+template <int R, bool TAB>
 cudaError_t launch_r(Stage1Args &a, const Stage1Plan &p, cudaStream_t st) {
     void *args[] = {&a};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void *)stage1_kernel<R>, dim3(p.blocks), dim3(kWarps * 32),
-                                                args, 0, st);
+    cudaError_t e = cudaLaunchCooperativeKernel((const void *)stage1_kernel<R, TAB>, dim3(p.blocks),
+                                                dim3(kWarps * 32), args, 0, st);
     if (e != cudaSuccess) return e;
     reduce_best_kernel<<<1, 256, 0, st>>>(a.wbest, (int64_t)p.blocks * kWarps, a.best);
     return cudaGetLastError();
 }
 
-template <int R>
+template <int R, bool TAB>
 int max_blocks_r() {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, stage1_kernel<R>, kWarps * 32, 0) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, stage1_kernel<R, TAB>, kWarps * 32, 0) != cudaSuccess)
+        return 0;
     return nb;
 }
 
 }  // namespace
 
-int stage1_max_blocks_per_sm(int R, int warps_per_block) {
-    (void)warps_per_block;
+int stage1_max_blocks_per_sm(int R, bool tab) {
     switch (R) {
-        case 8: return max_blocks_r<8>();
-        case 16: return max_blocks_r<16>();
-        case 32: return max_blocks_r<32>();
+        case 8: return tab ? max_blocks_r<8, true>() : max_blocks_r<8, false>();
+        case 16: return tab ? max_blocks_r<16, true>() : max_blocks_r<16, false>();
+        case 32: return tab ? max_blocks_r<32, true>() : max_blocks_r<32, false>();
         default: return 0;
     }
 }
 
-Stage1Plan stage1_plan(int64_t m, int64_t n, int device_sms, int R_hint) {
+Stage1Plan stage1_plan(int64_t m, int64_t n, int device_sms, int R_hint, bool tab) {
     Stage1Plan p;
-    p.R = (R_hint == 8 || R_hint == 16 || R_hint == 32) ? R_hint : 32;
+    p.R = (R_hint == 8 || R_hint == 16 || R_hint == 32) ? R_hint : 16;
+    p.tab = tab;
     p.warps_per_block = kWarps;
     p.strip_rows = 32LL * p.R;
     p.nstrips = (m + p.strip_rows - 1) / p.strip_rows;
-    const int per_sm = stage1_max_blocks_per_sm(p.R, p.warps_per_block);
+    const int per_sm = stage1_max_blocks_per_sm(p.R, tab);
     const int64_t max_blocks = (int64_t)device_sms * (per_sm > 0 ? per_sm : 1);
     // enough blocks that every strip of the first round has a warp, spread over
     // whole multiples of the SM count when there is room
@@ -459,12 +531,41 @@ Stage1Plan stage1_plan(int64_t m, int64_t n, int device_sms, int R_hint) {
 }
 
 cudaError_t stage1_launch(Stage1Args &a, const Stage1Plan &p, cudaStream_t st) {
+    if (p.tab) {
+        switch (p.R) {
+            case 8: return launch_r<8, true>(a, p, st);
+            case 16: return launch_r<16, true>(a, p, st);
+            case 32: return launch_r<32, true>(a, p, st);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (p.R) {
-        case 8: return launch_r<8>(a, p, st);
-        case 16: return launch_r<16>(a, p, st);
-        case 32: return launch_r<32>(a, p, st);
+        case 8: return launch_r<8, false>(a, p, st);
+        case 16: return launch_r<16, false>(a, p, st);
+        case 32: return launch_r<32, false>(a, p, st);
         default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t stage1_presence(const uint8_t *seq, int64_t n, uint32_t *flags, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(flags, 0, 256 * sizeof(uint32_t), st);
+    if (e != cudaSuccess || n <= 0) return e;
+    int blocks = (int)std::min<int64_t>(1024, (n + 255) / 256);
+    presence_kernel<<<blocks, 256, 0, st>>>(seq, n, flags);
+    return cudaGetLastError();
+}
+
+cudaError_t stage1_encode(const uint8_t *rows, int64_t m, const uint8_t *cols, int64_t n, const uint8_t *d_lut,
+                          uint8_t *rcode, uint32_t *ctab, int32_t mt1, int32_t mm1, uint32_t *tab_hi,
+                          cudaStream_t st) {
+    const uint32_t mmb = (uint32_t)(uint8_t)(int8_t)mm1;
+    const uint32_t mm4 = mmb * 0x01010101u;
+    const uint32_t x1 = ((uint32_t)(uint8_t)(int8_t)mt1 ^ mmb) & 0xFFu;
+    *tab_hi = mm4;
+    int blocks = (int)std::min<int64_t>(4096, (std::max(m, n) + 255) / 256);
+    if (blocks < 1) blocks = 1;
+    encode_kernel<<<blocks, 256, 0, st>>>(rows, m, cols, n, d_lut, rcode, ctab, mm4, x1);
+    return cudaGetLastError();
 }
 
 uint64_t tie_key_host(const TieGeom &g, int64_t r, int64_t c) {

@@ -42,6 +42,9 @@ struct Stage1Args {
     int64_t m, n;
     int32_t open, ext, gx; // gap_open, gap_extend, max(gap_open, gap_extend)
     int32_t mt1, mm1;      // match - open, mismatch - open
+    const uint8_t *rcode;  // TAB mode: per-row code (0..3, 7 = matches nothing)
+    const uint32_t *ctab;  // TAB mode: per-column word of (s - open) bytes for codes 0..3
+    uint32_t tab_hi;       // TAB mode: (mismatch - open) in all four bytes (codes 4..7)
     int4 *hbuf;            // n entries {H + open, tag, F of the next row, tag}; 0xFF-filled per launch
     int2 *srows;           // special rows [nsr][n] of (H, F), or nullptr
     int64_t sr_every;      // a special row every sr_every strips
@@ -56,7 +59,8 @@ struct Stage1Args {
     int64_t nstrips;
     BestRec *wbest;        // one per warp of the grid
     BestRec *best;         // final reduced record
-    int32_t *err;          // [0] error code, [1] abort flag
+    int32_t *err;          // [0] error code, [1] abort flag, [2] best H seen so far (device-wide)
+    int64_t *trace;        // optional: per strip {start ns, end ns, SM id} (globaltimer)
     TieGeom tie;
 };
 
@@ -67,7 +71,8 @@ bool reference_geometry(int64_t rows, int64_t cols, int32_t *G, int32_t *T, int6
 
 // Stage-1 launch plan (chosen by the host for a pair).
 struct Stage1Plan {
-    int R = 32;            // rows per lane
+    bool tab = false;      // PRMT table substitution (column alphabet of <= 4 bytes)
+    int R = 16;            // rows per lane
     int warps_per_block = 4;
     int blocks = 0;
     int64_t strip_rows = 0;
@@ -79,8 +84,14 @@ struct Stage1Plan {
 // error (cudaSuccess on success); a bounded-wait timeout is reported through
 // a.err and *timed_out.
 cudaError_t stage1_launch(Stage1Args &a, const Stage1Plan &plan, cudaStream_t st);
-Stage1Plan stage1_plan(int64_t m, int64_t n, int device_sms, int R_hint);
-int stage1_max_blocks_per_sm(int R, int warps_per_block);
+Stage1Plan stage1_plan(int64_t m, int64_t n, int device_sms, int R_hint, bool tab);
+int stage1_max_blocks_per_sm(int R, bool tab);
+// 256 presence flags of the bytes of seq (device), for choosing TAB mode.
+cudaError_t stage1_presence(const uint8_t *seq, int64_t n, uint32_t *flags, cudaStream_t st);
+// TAB-mode encodings: rcode[m] and ctab[n] from a device byte->code table.
+cudaError_t stage1_encode(const uint8_t *rows, int64_t m, const uint8_t *cols, int64_t n, const uint8_t *d_lut,
+                          uint8_t *rcode, uint32_t *ctab, int32_t mt1, int32_t mm1, uint32_t *tab_hi,
+                          cudaStream_t st);
 
 uint64_t tie_key_host(const TieGeom &g, int64_t r, int64_t c);
 

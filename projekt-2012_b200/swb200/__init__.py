@@ -100,6 +100,8 @@ def lib():
         L.swb_version.restype = C.c_char_p
         L.swb_probe_cell_peak.argtypes = [C.c_int32] + [C.POINTER(C.c_double)] * 5
         L.swb_probe_cell_peak.restype = C.c_int
+        L.swb_probe_latency.argtypes = [C.c_int32, C.POINTER(C.c_double), C.c_int32]
+        L.swb_probe_latency.restype = C.c_int
         _lib = L
     return _lib
 
@@ -144,7 +146,7 @@ class Context:
     """One device context (owns a CUDA stream and reusable device buffers)."""
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, special_interval: int = 0,
-                 cuda_stream: int = 0):
+                 cuda_stream: int = 0, verbose: int = 0):
         L = lib()
         o = Options()
         L.swb_options_default(C.byref(o))
@@ -152,6 +154,7 @@ class Context:
         o.hbm_budget_bytes = hbm_budget_bytes
         o.special_interval = special_interval
         o.cuda_stream = cuda_stream
+        o.verbose = verbose
         h = C.c_void_p()
         rc = L.swb_ctx_create(C.byref(o), C.byref(h))
         if rc != SWB_OK:
@@ -213,6 +216,22 @@ class Context:
         finally:
             lib().swb_result_free(C.byref(r))
 
+    def trace(self):
+        """Stage-1 strip trace of the last call: numpy array [strips, 3] of
+        (start ns, end ns, SM id); needs Context(verbose=2)."""
+        import numpy as np
+        cnt = C.c_int64(0)
+        fn = lib().swb_trace_copy
+        fn.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
+        fn(self._h, None, 0, C.byref(cnt)) if False else None
+        probe = np.zeros(3, dtype=np.int64)
+        fn(self._h, probe.ctypes.data, 0, C.byref(cnt))
+        out = np.zeros((cnt.value, 3), dtype=np.int64)
+        rc = fn(self._h, out.ctypes.data, 3 * cnt.value, C.byref(cnt))
+        if rc != SWB_OK:
+            self._err(rc)
+        return out
+
     def special_row(self, idx: int, cols: int):
         import numpy as np
         out = np.zeros((cols, 2), dtype=np.int32)
@@ -243,3 +262,13 @@ def probe_cell_peak(device: int = 0) -> dict:
         raise SwbError(rc, "probe failed")
     return {"cells_per_s": v[0].value, "iadd_per_s": v[1].value, "viaddmax_per_s": v[2].value,
             "vimax3_per_s": v[3].value, "probe_ms": v[4].value}
+
+
+def probe_latency(device: int = 0) -> dict:
+    """Dependent-chain latency in SM cycles per op (swb_probe_latency)."""
+    v = (C.c_double * 6)()
+    rc = lib().swb_probe_latency(device, v, 6)
+    if rc != SWB_OK:
+        raise SwbError(rc, "latency probe failed")
+    names = ["iadd", "max_add_c", "viaddmax", "vimax3", "viaddmax_relu", "max_c"]
+    return dict(zip(names, list(v)))
