@@ -58,17 +58,18 @@ enum : int32_t { kErrNone = 0, kErrTimeout = 4 };
 __device__ __forceinline__ int32_t ld_volatile(const int32_t *p) {
     return *reinterpret_cast<const volatile int32_t *>(p);
 }
+// LL loads/stores are volatile asm (never removed, merged or reordered with
+// each other); they carry no "memory" clobber so the compiler may keep the
+// kernel's scalar parameters in registers across them.
 __device__ __forceinline__ int4 ld_ll(const int4 *p) {
     int4 v;
     asm volatile("ld.volatile.global.v4.s32 {%0,%1,%2,%3}, [%4];"
                  : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-                 : "l"(p)
-                 : "memory");
+                 : "l"(p));
     return v;
 }
 __device__ __forceinline__ void st_ll(int4 *p, int32_t ho, int32_t f, int32_t tag) {
-    asm volatile("st.volatile.global.v4.s32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(ho), "r"(tag), "r"(f), "r"(tag)
-                 : "memory");
+    asm volatile("st.volatile.global.v4.s32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(ho), "r"(tag), "r"(f), "r"(tag));
 }
 // Byte permute with per-nibble sign replication (PTX prmt default mode).
 __device__ __forceinline__ int32_t prmt(uint32_t lo, uint32_t hi, uint32_t sel) {
@@ -77,7 +78,7 @@ __device__ __forceinline__ int32_t prmt(uint32_t lo, uint32_t hi, uint32_t sel) 
     return r;
 }
 
-__device__ __noinline__ uint64_t tie_key(const TieGeom g, int64_t r, int64_t c) {
+__device__ __forceinline__ uint64_t tie_key(const TieGeom g, int64_t r, int64_t c) {
     if (g.mode == kTieRowMajor) return ((uint64_t)r << 32) | (uint64_t)c;
     // rows and columns are below 2^31: 32-bit arithmetic
     const uint32_t T = (uint32_t)g.T, G = (uint32_t)g.G, C = (uint32_t)g.C;
@@ -102,8 +103,7 @@ struct Best {
 };
 
 // Rows of `mask` hold the column maximum cm at column j: keep the smallest key.
-// Out of line, so the hot loop keeps only the threshold in a register.
-__device__ __noinline__ int32_t slow_best(uint32_t mask, int32_t cm, const TieGeom tie, int64_t m, int64_t r_origin,
+__device__ __forceinline__ int32_t slow_best(uint32_t mask, int32_t cm, const TieGeom tie, int64_t m, int64_t r_origin,
                                           int64_t c_origin, Best *b, int64_t row0, int32_t j, int32_t *gbest,
                                           int32_t open) {
     const int32_t before = b->ho;
@@ -147,48 +147,60 @@ struct StripCtx {
 
 // One anti-diagonal step.  PRED: some lanes of the warp are outside [0, n).
 // SC: this step may be a special-column step of some lane.
+//
+// Phase 1 computes, for every row of the lane, E and t = max(H_diag + s, E, 0)
+// (independent of the vertical chain); phase 2 runs the F chain and writes HO.
+// Every register of the lane arrays is read before it is overwritten, so no
+// copies are needed.  The column maximum is taken over t: a cell whose H comes
+// from F is strictly below the cell above it, so it can never hold the best
+// score, and a best cell always has H = t.
 template <int R, bool TAB, bool PRED, bool SC>
 __device__ __forceinline__ void step(Lane<R> &L, const Stage1Args &a, Best *b, const int4 *ring, int lane,
                                      const StripCtx &sc, int32_t k) {
     const int32_t j = k - lane;
     const bool act = !PRED || (j >= 0 && j < sc.n);
     const uint32_t cb = L.inB;
+    int32_t to[R];
     int32_t hod = (PRED && j == 0) ? L.hodInit : L.hodPrev;
-    int32_t f = L.inF;
-    int32_t flast = 0;
 #pragma unroll
     for (int i = 0; i < R; ++i) {
         int32_t s1;
         if (TAB) s1 = prmt(cb, a.tab_hi, L.ra[i]);
         else s1 = (L.ra[i] == cb) ? a.mt1 : a.mm1;
         const int32_t e = __viaddmax_s32(L.E[i], a.ext, L.HO[i]);
-        const int32_t t = __viaddmax_s32_relu(hod, s1, e);
-        const int32_t to = t + a.open;
-        const int32_t ho = __viaddmax_s32(f, a.open, to);
-        flast = f;
-        f = __viaddmax_s32(f, a.gx, to);
+        to[i] = __viaddmax_s32_relu(hod, s1, e) + a.open;
         hod = L.HO[i];
-        if (act) {
-            L.HO[i] = ho;
-            L.E[i] = e;
+        if (act) L.E[i] = e;
+    }
+    // column maximum of t as a shallow tree (branch input ready early)
+    int32_t cm;
+    {
+        int32_t l1[(R + 2) / 3];
+#pragma unroll
+        for (int q = 0; q < (R + 2) / 3; ++q) {
+            const int i = 3 * q;
+            l1[q] = (i + 2 < R) ? __vimax3_s32(to[i], to[i + 1], to[i + 2]) : (i + 1 < R ? max(to[i], to[i + 1]) : to[i]);
         }
+        constexpr int N1 = (R + 2) / 3;
+        int32_t l2[(N1 + 2) / 3];
+#pragma unroll
+        for (int q = 0; q < (N1 + 2) / 3; ++q) {
+            const int i = 3 * q;
+            l2[q] = (i + 2 < N1) ? __vimax3_s32(l1[i], l1[i + 1], l1[i + 2]) : (i + 1 < N1 ? max(l1[i], l1[i + 1]) : l1[i]);
+        }
+        constexpr int N2 = (N1 + 2) / 3;
+        cm = l2[0];
+#pragma unroll
+        for (int q = 1; q < N2; ++q) cm = max(cm, l2[q]);
     }
-    int32_t cm = L.HO[0];
+    int32_t f = L.inF;
+    int32_t flast = 0;
 #pragma unroll
-    for (int i = 1; i + 1 < R; i += 2) cm = __vimax3_s32(cm, L.HO[i], L.HO[i + 1]);
-    if (R % 2 == 0) cm = max(cm, L.HO[R - 1]);
-    if (act && cm >= L.thr) {
-        uint32_t mask = 0;
-#pragma unroll
-        for (int i = 0; i < R; ++i) mask |= (L.HO[i] == cm ? 1u : 0u) << i;
-        L.bho = slow_best(mask, cm, a.tie, a.m, a.r_origin, a.c_origin, b, sc.row0, j, a.err + 2, a.open);
-        L.thr = max(L.thr, L.bho);
-    }
-    if (SC && act && ((j + 1) & (a.sc_every - 1)) == 0) {
-        int2 *dst = a.scols + (int64_t)((j + 1) / a.sc_every - 1) * a.m + sc.row0;
-#pragma unroll
-        for (int i = 0; i < R; ++i)
-            if (sc.row0 + i < a.m) dst[i] = make_int2(L.HO[i] - a.open, L.E[i]);
+    for (int i = 0; i < R; ++i) {
+        const int32_t ho = __viaddmax_s32(f, a.open, to[i]);
+        flast = f;
+        f = __viaddmax_s32(f, a.gx, to[i]);
+        if (act) L.HO[i] = ho;
     }
 
     // outputs toward the lane below; lane 31 hands its slot to lane 0
@@ -206,6 +218,22 @@ __device__ __forceinline__ void step(Lane<R> &L, const Stage1Args &a, Best *b, c
     L.inHO = __shfl_sync(0xffffffffu, oHO, src);
     L.inF = __shfl_sync(0xffffffffu, oF, src);
     L.inB = __shfl_sync(0xffffffffu, oB, src);
+
+    if (act && cm >= L.thr) {
+        // rows holding cm in H: every row whose H = t = cm is among them (a row
+        // with HO == cm but t < cm takes H from F and can never be the best)
+        uint32_t mask = 0;
+#pragma unroll
+        for (int i = 0; i < R; ++i) mask |= (L.HO[i] == cm ? 1u : 0u) << i;
+        L.bho = slow_best(mask, cm, a.tie, a.m, a.r_origin, a.c_origin, b, sc.row0, j, a.err + 2, a.open);
+        L.thr = max(L.thr, L.bho);
+    }
+    if (SC && act && ((j + 1) & (a.sc_every - 1)) == 0) {
+        int2 *dst = a.scols + (int64_t)((j + 1) / a.sc_every - 1) * a.m + sc.row0;
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+            if (sc.row0 + i < a.m) dst[i] = make_int2(L.HO[i] - a.open, L.E[i]);
+    }
 }
 
 // Column value of column c: the table word (TAB) or the byte (CMP).
@@ -260,10 +288,12 @@ __device__ __forceinline__ bool commit(const Stage1Args &a, int4 *ring, int32_t 
 // (prefetched one refill ago) and prefetch columns [k+2kCH, k+3kCH).
 template <bool TAB>
 __device__ __forceinline__ bool refill(const Stage1Args &a, int4 *ring, int lane, int32_t strip, int32_t n,
-                                       int32_t k, Pre &pre, int32_t &thr, int32_t bho) {
+                                       int32_t k, Pre &pre, int32_t &thr, int32_t bho, int32_t &gpre) {
     // cells below the best H found anywhere so far can never win: raise the
-    // candidate threshold to it (ties at that value are still examined)
-    thr = max(bho, ld_volatile(a.err + 2) + a.open);
+    // candidate threshold to it (ties at that value are still examined); the
+    // value was loaded one refill ago
+    thr = max(bho, max(thr, gpre + a.open));
+    gpre = ld_volatile(a.err + 2);
     bool ok = true;
     if (lane < kCH) {
         const int32_t c = k + kCH + lane;
@@ -287,7 +317,8 @@ __device__ bool run_strip(const Stage1Args &a, int4 *ring, int lane, int32_t s, 
     sc.sr = a.srows != nullptr && ((int64_t)(s + 1) % a.sr_every) == 0 && (int64_t)(s + 1) * H <= a.m;
     sc.sr_off = sc.sr ? ((int64_t)(s + 1) / a.sr_every - 1) * a.n : 0;
     L.bho = bho;
-    L.thr = max(bho, ld_volatile(a.err + 2) + a.open);
+    int32_t gpre = ld_volatile(a.err + 2);
+    L.thr = max(bho, gpre + a.open);
 #pragma unroll
     for (int i = 0; i < R; ++i) {
         const int64_t r = sc.row0 + i;
@@ -349,12 +380,12 @@ __device__ bool run_strip(const Stage1Args &a, int4 *ring, int lane, int32_t s, 
     if (n > 32) kB = 32 + ((n - 32) / kCH) * kCH;
     int32_t k = 0;
     for (; k < kA; ++k) {
-        if (k > 0 && (k % kCH) == 0 && !refill<TAB>(a, ring, lane, s, n, k, pre, L.thr, L.bho)) return false;
+        if (k > 0 && (k % kCH) == 0 && !refill<TAB>(a, ring, lane, s, n, k, pre, L.thr, L.bho, gpre)) return false;
         if (a.scols) step<R, TAB, true, true>(L, a, b, ring, lane, sc, k);
         else step<R, TAB, true, false>(L, a, b, ring, lane, sc, k);
     }
     while (k < kB) {
-        if (!refill<TAB>(a, ring, lane, s, n, k, pre, L.thr, L.bho)) return false;
+        if (!refill<TAB>(a, ring, lane, s, n, k, pre, L.thr, L.bho, gpre)) return false;
         // lane l stores special column j = q*sc_every - 1 at step j + l: a chunk of
         // steps [k, k+kCH) needs the check when some (t + 1) mod sc_every < 32
         const bool sc_window = a.scols != nullptr && ((k + kCH) & (a.sc_every - 1)) < 32 + kCH;
@@ -366,7 +397,7 @@ __device__ bool run_strip(const Stage1Args &a, int4 *ring, int lane, int32_t s, 
         k += kCH;
     }
     for (; k < kEnd; ++k) {
-        if ((k % kCH) == 0 && !refill<TAB>(a, ring, lane, s, n, k, pre, L.thr, L.bho)) return false;
+        if ((k % kCH) == 0 && !refill<TAB>(a, ring, lane, s, n, k, pre, L.thr, L.bho, gpre)) return false;
         if (a.scols) step<R, TAB, true, true>(L, a, b, ring, lane, sc, k);
         else step<R, TAB, true, false>(L, a, b, ring, lane, sc, k);
     }
