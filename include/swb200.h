@@ -94,7 +94,7 @@ typedef struct {
 
 typedef struct {
     int32_t  device;                /* CUDA device ordinal                           */
-    uint64_t hbm_budget_bytes;      /* cap on special rows + sequences; 0 = 40 GiB  */
+    uint64_t hbm_budget_bytes;      /* cap on special rows/columns; 0 = 64 GiB      */
     int32_t  special_interval;      /* special-row spacing in rows; 0 = autotune    */
     int32_t  verbose;               /* bit 0: progress lines on stderr; bit 1: record
                                        the stage-1 strip trace (swb_trace_copy)     */

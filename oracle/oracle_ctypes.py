@@ -61,6 +61,11 @@ def lib():
                                     C.c_int64, C.c_int64, C.c_char_p, C.c_int64,
                                     C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         L.orc_traceback.restype = C.c_int64
+        L.orc_traceback_xp.argtypes = [u8p, C.c_int64, u8p, C.c_int64, C.POINTER(Scoring),
+                                       C.c_int64, C.c_int64, C.c_char_p, C.c_int64,
+                                       C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                       C.c_int64, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
+        L.orc_traceback_xp.restype = C.c_int64
         L.orc_score_ops.argtypes = [u8p, u8p, C.POINTER(Scoring), C.c_int64, C.c_int64,
                                     C.c_char_p, C.c_int64]
         L.orc_score_ops.restype = C.c_int64
@@ -131,6 +136,22 @@ def traceback(rows: bytes, cols: bytes, sc: Scoring, er: int, ec: int):
     if k < 0:
         raise RuntimeError(f"orc_traceback failed: {k}")
     return buf.raw[:k].decode(), sr.value, scol.value
+
+
+def traceback_xp(rows: bytes, cols: bytes, sc: Scoring, er: int, ec: int, interval: int):
+    """Returns (ops, start_row, start_col, [(row, col, score, gap), ...] top to bottom)."""
+    import numpy as np
+    cap = len(rows) + len(cols) + 8
+    buf = C.create_string_buffer(cap)
+    sr, scol, nx = C.c_int64(0), C.c_int64(0), C.c_int64(0)
+    xcap = len(rows) // max(1, interval) + 8
+    xs = np.zeros(4 * xcap, dtype=np.int64)
+    k = lib().orc_traceback_xp(rows, len(rows), cols, len(cols), C.byref(sc), er, ec, buf, cap,
+                               C.byref(sr), C.byref(scol), interval, xs.ctypes.data, xcap, C.byref(nx))
+    if k < 0:
+        raise RuntimeError(f"orc_traceback_xp failed: {k}")
+    xps = [tuple(int(v) for v in xs[4 * i:4 * i + 4]) for i in range(nx.value)]
+    return buf.raw[:k].decode(), sr.value, scol.value, xps
 
 
 def score_ops(rows: bytes, cols: bytes, sc: Scoring, sr: int, scol: int, ops: str) -> int:

@@ -360,6 +360,13 @@ enum { SRC_ZERO = 0, SRC_DIAG = 1, SRC_E = 2, SRC_F = 3,
 int64_t orc_traceback(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
                       const orc_scoring *sc, int64_t er, int64_t ec,
                       char *ops, int64_t cap, int64_t *sr, int64_t *sc_) {
+    return orc_traceback_xp(a, m, b, n, sc, er, ec, ops, cap, sr, sc_, 0, NULL, 0, NULL);
+}
+
+int64_t orc_traceback_xp(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
+                         const orc_scoring *sc, int64_t er, int64_t ec,
+                         char *ops, int64_t cap, int64_t *sr, int64_t *sc_,
+                         int64_t xp_interval, int64_t *xps, int64_t xp_cap, int64_t *nxp) {
     if (er < 0 || ec < 0 || er >= m || ec >= n) return -2;
     const int64_t rows = er + 1, cols = ec + 1;       /* the path stays above-left */
     if ((double)rows * (double)cols > 4.0e9) return -1;
@@ -404,6 +411,20 @@ int64_t orc_traceback(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
     int64_t r = er, c = ec, k = 0;
     int state = 0;                                    /* 0 = H, 1 = E, 2 = F */
     int64_t ret = -1;
+    int64_t suffix = 0, nx = 0;                       /* score of the path after the current cell */
+    /* crosspoint: the path's last cell on a row X with (X + 1) % xp_interval == 0,
+     * i.e. the cell entered when the walk moves up from row X + 1; its forward
+     * value is endH - suffix, gap = 1 when it is entered inside a vertical gap */
+#define ORC_XP(rr, cc, gapflag)                                                       \
+    do {                                                                              \
+        if (xp_interval > 0 && ((rr) + 1) % xp_interval == 0 && (rr) >= 0 && xps) {  \
+            if (nx < xp_cap) {                                                        \
+                xps[4 * nx] = (rr); xps[4 * nx + 1] = (cc);                           \
+                xps[4 * nx + 2] = endH - suffix; xps[4 * nx + 3] = (gapflag);         \
+            }                                                                         \
+            ++nx;                                                                     \
+        }                                                                             \
+    } while (0)
     for (;;) {
         if (r < 0 || c < 0) { ret = -2; break; }
         const uint8_t v = fl[r * cols + c];
@@ -412,8 +433,10 @@ int64_t orc_traceback(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
             if (src == SRC_DIAG) {
                 if (k >= cap) { ret = -1; break; }
                 ops[k++] = 'M';
+                suffix += (a[r] == b[c]) ? sc->match : sc->mismatch;
                 if ((v & BIT_DIAG_ZERO) || r == 0 || c == 0) { *sr = r; *sc_ = c; ret = k; break; }
                 --r; --c;
+                ORC_XP(r, c, 0);
             } else if (src == SRC_E) {
                 state = 1;
             } else if (src == SRC_F) {
@@ -422,14 +445,25 @@ int64_t orc_traceback(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
         } else if (state == 1) {
             if (k >= cap) { ret = -1; break; }
             ops[k++] = 'I';
+            suffix += (v & BIT_E_EXT) ? sc->gap_extend : sc->gap_open;
             state = (v & BIT_E_EXT) ? 1 : 0;
             --c;
         } else {
             if (k >= cap) { ret = -1; break; }
             ops[k++] = 'D';
+            suffix += (v & BIT_F_EXT) ? sc->gap_extend : sc->gap_open;
             state = (v & BIT_F_EXT) ? 2 : 0;
             --r;
+            ORC_XP(r, c, state == 2 ? 1 : 0);
         }
+    }
+#undef ORC_XP
+    if (nxp) *nxp = nx;
+    if (xps && nx > 1) {                              /* report top to bottom */
+        for (int64_t i = 0, j = (nx < xp_cap ? nx : xp_cap) - 1; i < j; ++i, --j)
+            for (int q = 0; q < 4; ++q) {
+                int64_t t = xps[4 * i + q]; xps[4 * i + q] = xps[4 * j + q]; xps[4 * j + q] = t;
+            }
     }
     free(fl);
     if (ret > 0) {                                    /* reverse to start -> end */
@@ -444,16 +478,19 @@ int64_t orc_score_ops(const uint8_t *a, const uint8_t *b, const orc_scoring *sc,
                       int64_t sr, int64_t sc_, const char *ops, int64_t nops) {
     int64_t r = sr, c = sc_, s = 0;
     char prev = 'M';
+    /* the recurrence lets a gap run restart through H, so each character after
+     * the first costs the better of extend and open */
+    const int32_t cont = sc->gap_extend > sc->gap_open ? sc->gap_extend : sc->gap_open;
     for (int64_t i = 0; i < nops; ++i) {
         const char o = ops[i];
         if (o == 'M') {
             s += (a[r] == b[c]) ? sc->match : sc->mismatch;
             ++r; ++c;
         } else if (o == 'I') {
-            s += (prev == 'I') ? sc->gap_extend : sc->gap_open;
+            s += (prev == 'I') ? cont : sc->gap_open;
             ++c;
         } else if (o == 'D') {
-            s += (prev == 'D') ? sc->gap_extend : sc->gap_open;
+            s += (prev == 'D') ? cont : sc->gap_open;
             ++r;
         } else {
             return INT64_MIN;

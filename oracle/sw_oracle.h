@@ -72,7 +72,19 @@ int64_t orc_traceback(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
                       const orc_scoring *sc, int64_t er, int64_t ec,
                       char *ops, int64_t cap, int64_t *sr, int64_t *sc_);
 
-/* Score of an alignment given as ops from (sr, sc_) (checks a traceback). */
+/* The same traceback, also reporting the path's crosspoints: for every row X
+ * with (X + 1) % xp_interval == 0 that the path crosses, the last path cell on
+ * row X (the cell the backward walk enters from row X + 1) as (X, col, forward
+ * value of the path at that cell, gap) where gap = 1 when the vertical gap
+ * continues across the row boundary; top to bottom, count in *nxp. */
+int64_t orc_traceback_xp(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
+                         const orc_scoring *sc, int64_t er, int64_t ec,
+                         char *ops, int64_t cap, int64_t *sr, int64_t *sc_,
+                         int64_t xp_interval, int64_t *xps, int64_t xp_cap, int64_t *nxp);
+
+/* Score of an alignment given as ops from (sr, sc_) (checks a traceback); a run
+ * of L same-direction gap characters costs gap_open + (L-1) * max(gap_open,
+ * gap_extend), which is what the recurrence gives. */
 int64_t orc_score_ops(const uint8_t *a, const uint8_t *b, const orc_scoring *sc,
                       int64_t sr, int64_t sc_, const char *ops, int64_t nops);
 

@@ -54,6 +54,7 @@ struct swb_ctx {
     int sms = 0;
     std::string err;
     DevBuf rows, cols, hbuf, wbest, best, errf, srows, scols, work, flags, lut, rcode, ctab, trace;
+    DevBuf tb[9];  // traceback scratch (ops, crosspoints, state, level-2 stores, recompute buffers)
     int64_t last_nstrips = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::mutex mu;
@@ -120,7 +121,7 @@ int swb_ctx_create(const swb_options *opts, swb_ctx **out) {
     if (!c) return fail(nullptr, SWB_ENOMEM, "swb_ctx_create: out of host memory");
     if (opts) c->opts = *opts;
     else swb_options_default(&c->opts);
-    if (c->opts.hbm_budget_bytes == 0) c->opts.hbm_budget_bytes = 40ULL << 30;
+    if (c->opts.hbm_budget_bytes == 0) c->opts.hbm_budget_bytes = 64ULL << 30;
     c->device = c->opts.device;
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -157,6 +158,7 @@ void swb_ctx_destroy(swb_ctx *c) {
     for (DevBuf *b : {&c->rows, &c->cols, &c->hbuf, &c->wbest, &c->best, &c->errf, &c->srows, &c->scols,
                       &c->work, &c->flags, &c->lut, &c->rcode, &c->ctab, &c->trace})
         b->release();
+    for (DevBuf &b : c->tb) b.release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
@@ -223,11 +225,12 @@ int check_scoring(swb_ctx *c, const swb_scoring *sc, int64_t rows, int64_t cols)
 
 // Runs stage 1 on device sequences already in the context's buffers.
 int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_cols, int64_t n,
-               const swb_scoring *sc, uint32_t flags, int64_t sr_interval_rows, swb::BestRec *best_out,
-               float *ms_out, int64_t *nsr_out) {
+               const swb_scoring *sc, uint32_t flags, int64_t sr_interval_rows, int64_t sc_interval,
+               swb::BestRec *best_out, float *ms_out, int64_t *nsr_out) {
     using namespace swb;
     int R = 16;
     if (const char *rv = std::getenv("SWB_STAGE1_R")) R = std::atoi(rv);  // tuning override: 8, 16 or 32
+    if (sr_interval_rows > 0 && (R > 16 || sr_interval_rows % (32 * R) != 0)) R = 16;  // strips must tile the rows
     cudaError_t e;
     // TAB mode when the column sequence has at most four distinct bytes and the
     // shifted scores fit a signed byte
@@ -292,19 +295,39 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
             return cuda_fail(c, e, "trace buffer");
         a.trace = (int64_t *)c->trace.p;
     }
+    a.scols = nullptr;
+    a.sc_every = 1 << 30;
+    a.nsc = 0;
+    size_t sbytes = 0;
     if (sr_interval_rows > 0) {
         const int64_t every = std::max<int64_t>(1, sr_interval_rows / plan.strip_rows);
         const int64_t nsr = (m / plan.strip_rows) / every;
+        sbytes += sizeof(int2) * (size_t)nsr * (size_t)n;
         if (nsr > 0) {
-            const size_t bytes = sizeof(int2) * (size_t)nsr * (size_t)n;
-            if (bytes > c->opts.hbm_budget_bytes)
-                return fail(c, SWB_ENOMEM_BUDGET, "special rows need %zu bytes > budget %llu", bytes,
-                            (unsigned long long)c->opts.hbm_budget_bytes);
-            if ((e = c->srows.ensure(bytes)) != cudaSuccess) return cuda_fail(c, e, "special rows");
-            a.srows = (int2 *)c->srows.p;
             a.sr_every = every;
             a.nsr = nsr;
         }
+    }
+    if (sc_interval > 0) {
+        const int64_t nsc = n / sc_interval;
+        sbytes += sizeof(int2) * (size_t)nsc * (size_t)m;
+        if (nsc > 0) {
+            a.sc_every = (int32_t)sc_interval;
+            a.nsc = nsc;
+        }
+    }
+    if (sbytes > c->opts.hbm_budget_bytes)
+        return fail(c, SWB_ENOMEM_BUDGET, "special rows and columns need %zu bytes > budget %llu", sbytes,
+                    (unsigned long long)c->opts.hbm_budget_bytes);
+    if (a.nsr > 0) {
+        if ((e = c->srows.ensure(sizeof(int2) * (size_t)a.nsr * (size_t)n)) != cudaSuccess)
+            return cuda_fail(c, e, "special rows");
+        a.srows = (int2 *)c->srows.p;
+    }
+    if (a.nsc > 0) {
+        if ((e = c->scols.ensure(sizeof(int2) * (size_t)a.nsc * (size_t)m)) != cudaSuccess)
+            return cuda_fail(c, e, "special columns");
+        a.scols = (int2 *)c->scols.p;
     }
     c->last_nsr = a.nsr;
     c->last_n = n;
@@ -337,8 +360,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
 }
 
 int align_device(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_cols, int64_t n,
-                 const swb_scoring *sc, uint32_t flags, swb_result *out, int swapped,
-                 const uint8_t *h_rows, const uint8_t *h_cols) {
+                 const swb_scoring *sc, uint32_t flags, swb_result *out, int swapped) {
     using namespace swb;
     const auto t0 = std::chrono::steady_clock::now();
     std::memset(out, 0, sizeof *out);
@@ -354,17 +376,24 @@ int align_device(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_
         return SWB_OK;
     }
     const bool score_only = (flags & SWB_FLAG_SCORE_ONLY) != 0;
-    int64_t sr_interval = 0;
-    if (!(flags & SWB_FLAG_NO_SPECIAL)) sr_interval = tb::choose_special_interval(c->opts, m, n);
+    tb::Plan plan;
+    int64_t sr_interval = 0, sc_interval = 0;
+    if (!score_only) {
+        plan = tb::plan_for(c->opts, m, n);
+        sr_interval = plan.kr;
+        sc_interval = plan.kc;
+    } else if (c->opts.special_interval > 0 && !(flags & SWB_FLAG_NO_SPECIAL)) {
+        sr_interval = c->opts.special_interval;  // inspection of special rows only
+    }
     BestRec best{};
     float ms = 0.f;
     int64_t nsr = 0;
-    int rc = run_stage1(c, d_rows, m, d_cols, n, sc, flags, sr_interval, &best, &ms, &nsr);
+    int rc = run_stage1(c, d_rows, m, d_cols, n, sc, flags, sr_interval, sc_interval, &best, &ms, &nsr);
     if (rc != SWB_OK) return rc;
     out->stage1_ms = ms;
     out->kernel_launches += c->last_launches;
     out->special_interval = (int32_t)c->last_sr_interval;
-    out->special_bytes = (int64_t)sizeof(int2) * nsr * n;
+    out->special_bytes = (int64_t)sizeof(int2) * nsr * n + (sc_interval > 0 ? (int64_t)sizeof(int2) * (n / sc_interval) * m : 0);
     if (best.valid) {
         out->score = best.ho - sc->gap_open;
         out->end_row = best.row;
@@ -378,10 +407,25 @@ int align_device(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_
     out->start_col = out->end_col;
     if (!score_only && out->score > 0) {
         const auto t1 = std::chrono::steady_clock::now();
-        rc = tb::traceback(c->stream, d_rows, m, d_cols, n, sc, (const int2 *)c->srows.p, nsr,
-                           c->last_sr_interval, out, h_rows, h_cols, c->err);
+        tb::Scratch scr;
+        scr.owner = c;
+        scr.ensure = [](void *owner, int which, size_t bytes) -> void * {
+            swb_ctx *cx = (swb_ctx *)owner;
+            return cx->tb[which].ensure(bytes) == cudaSuccess ? cx->tb[which].p : nullptr;
+        };
+        int32_t launches = 0;
+        rc = tb::traceback(c->stream, c->sms, d_rows, m, d_cols, n, sc, plan, (const int2 *)c->srows.p,
+                           (const int2 *)c->scols.p, out, scr, c->err, &launches);
         if (rc != SWB_OK) return fail(c, rc, "%s", c->err.c_str());
+        out->kernel_launches += launches;
         out->stage2_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
+    } else if (!score_only) {
+        // best score 0: empty alignment, crosspoints [start = end]
+        out->xpoints = (swb_xpoint *)std::malloc(sizeof(swb_xpoint) * 2);
+        if (out->xpoints) {
+            out->xpoints[0] = swb_xpoint{0, 0, out->end_row, out->end_col};
+            out->n_xpoints = 1;
+        }
     }
     out->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return SWB_OK;
@@ -399,8 +443,7 @@ extern "C" int swb_align_pair_device(swb_ctx *c, const void *d_rows, int64_t row
     if (rc != SWB_OK) return rc;
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
-    return align_device(c, (const uint8_t *)d_rows, rows, (const uint8_t *)d_cols, cols, sc, flags, out, 0, nullptr,
-                        nullptr);
+    return align_device(c, (const uint8_t *)d_rows, rows, (const uint8_t *)d_cols, cols, sc, flags, out, 0);
 }
 
 extern "C" int swb_align_pair(swb_ctx *c, const uint8_t *a, int64_t la, const uint8_t *b, int64_t lb,
@@ -424,8 +467,7 @@ extern "C" int swb_align_pair(swb_ctx *c, const uint8_t *a, int64_t la, const ui
         return cuda_fail(c, e, "copy rows");
     if (n > 0 && (e = cudaMemcpyAsync(c->cols.p, hc, (size_t)n, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
         return cuda_fail(c, e, "copy cols");
-    return align_device(c, (const uint8_t *)c->rows.p, m, (const uint8_t *)c->cols.p, n, sc, flags, out, swap ? 1 : 0,
-                        hr, hc);
+    return align_device(c, (const uint8_t *)c->rows.p, m, (const uint8_t *)c->cols.p, n, sc, flags, out, swap ? 1 : 0);
 }
 
 // Copies special row `idx` (row (idx+1)*interval - 1) of the last call as (H, F)

@@ -8,15 +8,60 @@
 namespace swb {
 namespace tb {
 
-// Special-row spacing (rows) for a pair under the context's HBM budget.
+// Special-row / special-column spacing of stage 1 for a pair.  Direct mode keeps
+// the walker's 512 x 256 grid; level-1 mode keeps a coarser grid that fits the
+// HBM budget and recomputes each level-1 cell on the path.
+struct Plan {
+    bool level1 = false;
+    int64_t kr = 512;   // special-row spacing (rows), multiple of 512
+    int64_t kc = 256;   // special-column spacing (columns), power of two >= 256
+};
+Plan plan_for(const swb_options &opts, int64_t m, int64_t n);
 int64_t choose_special_interval(const swb_options &opts, int64_t m, int64_t n);
 
+// Inputs of one walker launch over a region [rr0, rr1) x [cc0, cc1).
+struct WalkInputs {
+    const uint8_t *rows, *cols;   // whole sequences (device)
+    int64_t m, n;
+    swb_scoring sc;
+    int32_t score;
+    const int2 *srows, *scols;    // the region's 512 x 256 stores
+    int64_t rr0, cc0, rr1, cc1;
+    const int2 *rtop, *rleft;     // region boundary (nullptr = matrix edge)
+    int32_t rcorner;
+    int32_t xp_interval;
+    char *ops;
+    int64_t ops_cap;
+    int64_t *xps;
+    int64_t xp_cap;
+    int64_t *dstate;              // device copy of the walker state
+};
+int walk_region(cudaStream_t st, const WalkInputs &in, int64_t *host_state, std::string &err);
+int state_slots();
+int slot_r();
+int slot_c();
+int slot_state();
+int slot_nops();
+int slot_nxp();
+int slot_done();
+int slot_start_r();
+int slot_start_c();
+int block_rows();
+int block_cols();
+
+// Device scratch the orchestration needs (owned by the caller's context).
+struct Scratch {
+    void *(*ensure)(void *owner, int which, size_t bytes);  // returns device memory or nullptr
+    void *owner;
+};
+enum ScratchSlot { kScrOps = 0, kScrXps, kScrState, kScrSrows2, kScrScols2, kScrHbuf, kScrWbest, kScrBest, kScrErr };
+
 // Canonical traceback from the end cell in `out` (score, end_row, end_col set by
-// stage 1).  Fills out->ops / out->n_ops / start_* / xpoints.  Returns SWB_OK or
-// an SWB_E* code with `err` set.
-int traceback(cudaStream_t st, const uint8_t *d_rows, int64_t m, const uint8_t *d_cols, int64_t n,
-              const swb_scoring *sc, const int2 *d_srows, int64_t nsr, int64_t sr_interval, swb_result *out,
-              const uint8_t *h_rows, const uint8_t *h_cols, std::string &err);
+// stage 1), using the stage-1 stores laid out by `plan`.  Fills out->ops,
+// out->n_ops, start_*, xpoints.  Returns SWB_OK or an SWB_E* code with `err`.
+int traceback(cudaStream_t st, int sms, const uint8_t *d_rows, int64_t m, const uint8_t *d_cols, int64_t n,
+              const swb_scoring *sc, const Plan &plan, const int2 *d_srows, const int2 *d_scols, swb_result *out,
+              const Scratch &scr, std::string &err, int32_t *launches);
 
 }  // namespace tb
 }  // namespace swb

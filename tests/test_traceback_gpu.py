@@ -1,0 +1,122 @@
+"""Stage 2 on the GPU (alignment ops, start cell, crosspoints) against the
+oracle's full-matrix traceback with the same precedence, through the C ABI."""
+import os
+import random
+import subprocess
+
+import pytest
+
+import oracle_ctypes as O
+import swb200
+from conftest import GOLDEN, load_fixture_fasta
+
+pytestmark = pytest.mark.gpu
+
+SCORINGS = [(1, -3, -5, -2), (5, -5, -5, -5), (2, -3, -5, -2), (1, -1, -1, -1), (3, -1, -1, -2), (2, -1, -1, -3)]
+
+
+def _expected(a, b, sc_t, interval):
+    rows, cols, swapped = O.orient(a, b)
+    sc = O.scoring(*sc_t)
+    e = O.stage1(rows, cols, sc, O.TEXTBOOK, O.TIE_REFERENCE)
+    if e.score == 0:
+        return e, "", e.row, e.col, []
+    ops, sr, scol, xps = O.traceback_xp(rows, cols, sc, e.row, e.col, interval)
+    return e, ops, sr, scol, xps
+
+
+def _check(ctx, a, b, sc_t):
+    r = ctx.align(a, b, swb200.scoring(*sc_t))
+    e, ops, sr, scol, xps = _expected(a, b, sc_t, r.xpoint_interval)
+    assert (r.score, r.end_row, r.end_col) == (e.score, e.row, e.col)
+    if e.score == 0:
+        assert r.ops == ""
+        return r
+    assert r.ops == ops, (len(a), len(b), sc_t)
+    assert (r.start_row, r.start_col) == (sr, scol)
+    # [start, crosspoints top -> bottom, end]
+    assert r.xpoints[0] == (sr, scol, 0, 0)
+    assert r.xpoints[-1] == (e.row, e.col, e.score, 0)
+    assert [(x[0], x[1], x[2], x[3]) for x in r.xpoints[1:-1]] == xps
+    return r
+
+
+def _similar_pair(rng, m, frac, sub=0.08, indel=0.02):
+    a = bytes(rng.choice(b"ACGT") for _ in range(m))
+    st = rng.randint(0, max(0, m - int(m * frac)))
+    out = bytearray()
+    for ch in a[st:st + int(m * frac)]:
+        x = rng.random()
+        if x < indel / 2:
+            continue
+        if x < indel:
+            out += bytes(rng.choice(b"ACGT") for _ in range(rng.randint(1, 6)))
+        out.append(rng.choice(b"ACGT") if rng.random() < sub else ch)
+    b = bytes(rng.choice(b"ACGT") for _ in range(rng.randint(0, 300))) + bytes(out) + \
+        bytes(rng.choice(b"ACGT") for _ in range(rng.randint(0, 300)))
+    return a, b
+
+
+def test_random_pairs_match_oracle(gpu_ctx):
+    rng = random.Random(404)
+    for _ in range(60):
+        alph = rng.choice([b"ACGT", b"AC", b"A"])
+        a = bytes(rng.choice(alph) for _ in range(rng.randint(1, 700)))
+        b = bytes(rng.choice(alph) for _ in range(rng.randint(1, 700)))
+        _check(gpu_ctx, a, b, rng.choice(SCORINGS))
+
+
+def test_similar_pairs_cross_many_blocks(gpu_ctx):
+    rng = random.Random(505)
+    for m in (1500, 3000, 5200):
+        a, b = _similar_pair(rng, m, 0.8)
+        for sc_t in SCORINGS[:3] + SCORINGS[4:]:
+            _check(gpu_ctx, a, b, sc_t)
+
+
+def test_level1_mode_matches_oracle():
+    """A tiny HBM budget forces the coarse store grid: level-1 cells are
+    recomputed by the stage-1 kernel on the GPU before the walk."""
+    rng = random.Random(606)
+    with swb200.Context(device=0, hbm_budget_bytes=1 << 20) as ctx:
+        for m in (2600, 6000):
+            a, b = _similar_pair(rng, m, 0.85)
+            r = _check(ctx, a, b, (1, -3, -5, -2))
+            assert r.kernel_launches > 4
+
+
+def test_reference_fixtures(gpu_ctx):
+    for fa, fb, sc_t in [("1/A00142.fna.gz", "1/A00145.fna.gz", (5, -5, -5, -5)),
+                         ("2/NC_005046.fna.gz", "2/NC_012557.fna.gz", (5, -5, -5, -5)),
+                         ("0/seq0.fna.gz", "0/seq1.fna.gz", (5, -5, -5, -5)),
+                         ("0/seq5.fna.gz", "0/seq6.fna.gz", (1, -3, -5, -2)),
+                         ("0/seq3.fna.gz", "0/seq4.fna.gz", (1, -3, -5, -2))]:
+        _check(gpu_ctx, load_fixture_fasta(fa), load_fixture_fasta(fb), sc_t)
+
+
+def test_long_alignment_is_optimal(gpu_ctx):
+    """100 kbp similar pair: the GPU alignment scores exactly the best score and
+    spans start..end (size-independent properties; no full-matrix oracle)."""
+    rng = random.Random(707)
+    a, b = _similar_pair(rng, 100_000, 0.9, sub=0.05, indel=0.01)
+    sc_t = (1, -3, -5, -2)
+    r = gpu_ctx.align(a, b, swb200.scoring(*sc_t))
+    rows, cols, _ = O.orient(a, b)
+    assert O.score_ops(rows, cols, O.scoring(*sc_t), r.start_row, r.start_col, r.ops) == r.score
+    assert r.start_row + r.ops.count("M") + r.ops.count("D") - 1 == r.end_row
+    assert r.start_col + r.ops.count("M") + r.ops.count("I") - 1 == r.end_col
+    assert r.score > 50_000
+
+
+def test_cli_prints_reference_lines(tmp_path):
+    fa = tmp_path / "a.fna"
+    fb = tmp_path / "b.fna"
+    import gzip
+    fa.write_bytes(gzip.open(os.path.join(GOLDEN, "seqs", "1", "A00142.fna.gz")).read())
+    fb.write_bytes(gzip.open(os.path.join(GOLDEN, "seqs", "1", "A00145.fna.gz")).read())
+    p = subprocess.run([swb200.CLI_PATH, str(fa), str(fb), "5", "-5", "-5", "-5"], capture_output=True, text=True)
+    assert p.returncode == 0, p.stdout + p.stderr
+    assert "\t>Alignment score: 480 at [623, 561]\n\n" in p.stdout
+    assert "\t>Cell updates per second: " in p.stdout
+    assert "Found " in p.stdout and "\t>xPoint[0]: [" in p.stdout
+    assert "Visual representation of the alignment" in p.stdout
