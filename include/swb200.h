@@ -172,6 +172,59 @@ int swb_score_pair_noalloc(int32_t device, const void *d_rows, int64_t rows, con
                            swb_score *out);
 const char *swb_noalloc_last_error(void);
 
+/* ---------------------------------------------------------------- batches
+ *
+ * Many independent pairs of uneven length in one persistent launch.  No
+ * counterpart in the reference, which aligns one pair per process run
+ * (src/main.cu:102-249); each pair gets exactly the result swb_align_pair()
+ * gives it alone (score, end cell, tie rule, alignment and crosspoints). */
+
+/* One pair of a batch: byte ranges of the batch's sequence buffer. */
+typedef struct {
+    int64_t a_off, a_len;
+    int64_t b_off, b_len;
+} swb_pair_ref;
+
+typedef struct {
+    int32_t score;
+    int32_t swapped;                /* 1: A was shorter and became cols             */
+    int64_t end_row, end_col;       /* 0-based, rows = longer sequence              */
+    int64_t start_row, start_col;   /* traced pairs; = end otherwise                */
+    int64_t ops_off, n_ops;         /* traced pairs: ops[ops_off, +n_ops) of the result */
+    int64_t xp_off, n_xpoints;      /* traced pairs: xpoints[xp_off, +n_xpoints)    */
+    int32_t traced;                 /* 1: alignment and crosspoints were computed   */
+    int32_t xpoint_interval;        /* reference special-row spacing of this pair   */
+} swb_batch_item;
+
+typedef struct {
+    int64_t npairs;
+    swb_batch_item *items;          /* in the order of the pairs argument           */
+    char *ops;                      /* 'M'/'I'/'D' of every traced pair             */
+    int64_t ops_bytes;
+    swb_xpoint *xpoints;            /* [start, crosspoints, end] of every traced pair */
+    int64_t n_xpoints;
+    int64_t n_traced;
+    int64_t cells;                  /* sum of rows * cols                           */
+    double stage1_ms;               /* device time of the batched scoring launch    */
+    double stage2_ms;               /* device + host time of the traced pairs       */
+    double total_ms;                /* wall time of the call                        */
+    int32_t kernel_launches;
+} swb_batch_result;
+
+/* Aligns npairs pairs whose sequences are byte ranges of the host buffer seq
+ * (seq_bytes long).  Scores and end cells of every pair; the alignment and
+ * crosspoints of the ceil(trace_frac * npairs) best-scoring pairs (ties: lower
+ * index first; trace_frac in [0, 1]).  flags: SWB_FLAG_TIE_ROWMAJOR.  Result
+ * buffers are library-owned until swb_batch_result_free(). */
+int swb_batch_align(swb_ctx *ctx, const uint8_t *seq, int64_t seq_bytes, const swb_pair_ref *pairs,
+                    int64_t npairs, const swb_scoring *sc, uint32_t flags, double trace_frac,
+                    swb_batch_result *out);
+/* Same with the sequence buffer already in device memory of the context's device. */
+int swb_batch_align_device(swb_ctx *ctx, const void *d_seq, int64_t seq_bytes, const swb_pair_ref *pairs,
+                           int64_t npairs, const swb_scoring *sc, uint32_t flags, double trace_frac,
+                           swb_batch_result *out);
+void swb_batch_result_free(swb_batch_result *res);
+
 /* Stage-1 strip trace of the context's last call when options.verbose has bit 1
  * set: per strip {start ns, end ns, SM id} from %globaltimer / %smid, written to
  * out[3*strips] (cap entries available); *count receives the strip count. */

@@ -15,55 +15,52 @@
 #include <string>
 #include <vector>
 
-#include "swb_internal.h"
+#include "ctx.h"
 #include "traceback.h"
 
 #define SWB_VERSION_STRING "swb200 0.1.0 (sm_100a)"
 
 namespace {
-
 thread_local std::string g_thread_err;
-
-struct DevBuf {
-    void *p = nullptr;
-    size_t cap = 0;
-    cudaError_t ensure(size_t bytes) {
-        if (bytes <= cap && p) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        size_t want = bytes < 256 ? 256 : bytes;
-        cudaError_t e = cudaMalloc(&p, want);
-        if (e == cudaSuccess) cap = want;
-        return e;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-    }
-};
-
 }  // namespace
 
-struct swb_ctx {
-    int device = 0;
-    swb_options opts{};
-    cudaStream_t stream = nullptr;
-    bool own_stream = true;
-    int sms = 0;
-    std::string err;
-    DevBuf rows, cols, hbuf, wbest, best, errf, srows, scols, work, flags, lut, rcode, ctab, trace;
-    DevBuf tb[9];  // traceback scratch (ops, crosspoints, state, level-2 stores, recompute buffers)
-    int64_t last_nstrips = 0;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::mutex mu;
-    // last stage-1 special-row layout (for swb_special_row_copy)
-    int64_t last_nsr = 0, last_n = 0, last_sr_interval = 0;
-    int32_t last_launches = 0;  // this library's kernels launched by the last stage 1
-};
+namespace swb {
 
-static int fail(swb_ctx *ctx, int code, const char *fmt, ...) {
+cudaError_t DevBuf::ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = bytes < 256 ? 256 : bytes;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+}
+
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+}
+
+cudaError_t HostBuf::ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = bytes < 4096 ? 4096 : bytes;
+    cudaError_t e = cudaMallocHost(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+}
+
+void HostBuf::release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+}
+
+int ctx_fail(swb_ctx *ctx, int code, const char *fmt, ...) {
     char buf[512];
     va_list ap;
     va_start(ap, fmt);
@@ -74,9 +71,15 @@ static int fail(swb_ctx *ctx, int code, const char *fmt, ...) {
     return code;
 }
 
-static int cuda_fail(swb_ctx *ctx, cudaError_t e, const char *what) {
-    return fail(ctx, SWB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+int ctx_cuda_fail(swb_ctx *ctx, cudaError_t e, const char *what) {
+    return ctx_fail(ctx, SWB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
 }
+
+}  // namespace swb
+
+using swb::ctx_fail;
+using swb::ctx_cuda_fail;
+using swb::DevBuf;
 
 namespace swb {
 
@@ -115,10 +118,10 @@ void swb_options_default(swb_options *o) {
 }
 
 int swb_ctx_create(const swb_options *opts, swb_ctx **out) {
-    if (!out) return fail(nullptr, SWB_EINVAL, "swb_ctx_create: out is NULL");
+    if (!out) return ctx_fail(nullptr, SWB_EINVAL, "swb_ctx_create: out is NULL");
     *out = nullptr;
     swb_ctx *c = new (std::nothrow) swb_ctx();
-    if (!c) return fail(nullptr, SWB_ENOMEM, "swb_ctx_create: out of host memory");
+    if (!c) return ctx_fail(nullptr, SWB_ENOMEM, "swb_ctx_create: out of host memory");
     if (opts) c->opts = *opts;
     else swb_options_default(&c->opts);
     if (c->opts.hbm_budget_bytes == 0) c->opts.hbm_budget_bytes = 64ULL << 30;
@@ -127,19 +130,19 @@ int swb_ctx_create(const swb_options *opts, swb_ctx **out) {
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev <= 0) {
         delete c;
-        return fail(nullptr, SWB_ECUDA, "no CUDA device: %s", cudaGetErrorString(e));
+        return ctx_fail(nullptr, SWB_ECUDA, "no CUDA device: %s", cudaGetErrorString(e));
     }
     if (c->device < 0 || c->device >= ndev) {
         const int dev = c->device;
         delete c;
-        return fail(nullptr, SWB_EINVAL, "device %d out of range (%d devices)", dev, ndev);
+        return ctx_fail(nullptr, SWB_EINVAL, "device %d out of range (%d devices)", dev, ndev);
     }
     if ((e = cudaSetDevice(c->device)) != cudaSuccess ||
         (e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device)) != cudaSuccess ||
         (c->opts.cuda_stream == 0 &&
          (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) ||
         (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess) {
-        int rc = cuda_fail(nullptr, e, "swb_ctx_create");
+        int rc = ctx_cuda_fail(nullptr, e, "swb_ctx_create");
         delete c;
         return rc;
     }
@@ -159,6 +162,11 @@ void swb_ctx_destroy(swb_ctx *c) {
                       &c->work, &c->flags, &c->lut, &c->rcode, &c->ctab, &c->trace})
         b->release();
     for (DevBuf &b : c->tb) b.release();
+    for (DevBuf *b : {&c->b_seq, &c->b_rcode, &c->b_ctab, &c->b_pairs, &c->b_units, &c->b_hbuf, &c->b_gbest,
+                      &c->b_ubest, &c->b_pbest, &c->b_ctl, &c->b_srows, &c->b_scols, &c->b_walk, &c->b_ops,
+                      &c->b_xps, &c->b_state})
+        b->release();
+    c->h_stage.release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
@@ -172,14 +180,14 @@ const char *swb_version(void) { return SWB_VERSION_STRING; }
 int swb_scoring_parse(const char *match, const char *mismatch, const char *gap_open, const char *gap_extend,
                       swb_scoring *out) {
     if (!match || !mismatch || !gap_open || !gap_extend || !out)
-        return fail(nullptr, SWB_EINVAL, "swb_scoring_parse: NULL argument");
+        return ctx_fail(nullptr, SWB_EINVAL, "swb_scoring_parse: NULL argument");
     swb_scoring s;
     s.match = std::atoi(match);
     s.mismatch = std::atoi(mismatch);
     s.gap_open = std::atoi(gap_open);
     s.gap_extend = std::atoi(gap_extend);
     if (s.match < 1 || s.mismatch > -1 || s.gap_open > -1 || s.gap_extend > -1)
-        return fail(nullptr, SWB_EINVAL, "One or more scoring values were not usable!");
+        return ctx_fail(nullptr, SWB_EINVAL, "One or more scoring values were not usable!");
     *out = s;
     return SWB_OK;
 }
@@ -212,14 +220,14 @@ namespace {
 // Scoring values must stay in the exact int32 range of the recurrence for the
 // lengths involved (|score| <= max(|s|) * (rows + cols)).
 int check_scoring(swb_ctx *c, const swb_scoring *sc, int64_t rows, int64_t cols) {
-    if (!sc) return fail(c, SWB_EINVAL, "scoring is NULL");
+    if (!sc) return ctx_fail(c, SWB_EINVAL, "scoring is NULL");
     if (sc->match < 1 || sc->mismatch > -1 || sc->gap_open > -1 || sc->gap_extend > -1)
-        return fail(c, SWB_EINVAL, "One or more scoring values were not usable!");
+        return ctx_fail(c, SWB_EINVAL, "One or more scoring values were not usable!");
     const long double worst = (long double)std::max<int64_t>(
                                   {(int64_t)sc->match, -(int64_t)sc->mismatch, -(int64_t)sc->gap_open,
                                    -(int64_t)sc->gap_extend}) *
                               (long double)(rows + cols + 2);
-    if (worst > 2.0e9L) return fail(c, SWB_EUNSUPPORTED, "scores would leave the int32 range");
+    if (worst > 2.0e9L) return ctx_fail(c, SWB_EUNSUPPORTED, "scores would leave the int32 range");
     return SWB_OK;
 }
 
@@ -245,7 +253,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
             (e = cudaMemcpyAsync(present, c->flags.p, sizeof present, cudaMemcpyDeviceToHost, c->stream)) !=
                 cudaSuccess ||
             (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
-            return cuda_fail(c, e, "column alphabet");
+            return ctx_cuda_fail(c, e, "column alphabet");
         c->last_launches += 1;
         int K = 0;
         for (int i = 0; i < 256; ++i) lut[i] = present[i] ? (uint8_t)(K++) : 7;
@@ -257,7 +265,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
         (e = c->wbest.ensure(sizeof(BestRec) * (size_t)W)) != cudaSuccess ||
         (e = c->best.ensure(sizeof(BestRec))) != cudaSuccess ||
         (e = c->errf.ensure(4 * sizeof(int32_t))) != cudaSuccess)
-        return cuda_fail(c, e, "stage 1 buffers");
+        return ctx_cuda_fail(c, e, "stage 1 buffers");
 
     Stage1Args a{};
     a.rows = d_rows;
@@ -275,7 +283,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
             (e = cudaMemcpyAsync(c->lut.p, lut, 256, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
             (e = stage1_encode(d_rows, m, d_cols, n, (const uint8_t *)c->lut.p, (uint8_t *)c->rcode.p,
                                (uint32_t *)c->ctab.p, mt1, mm1, &a.tab_hi, c->stream)) != cudaSuccess)
-            return cuda_fail(c, e, "stage 1 encode");
+            return ctx_cuda_fail(c, e, "stage 1 encode");
         c->last_launches += 1;
         a.rcode = (const uint8_t *)c->rcode.p;
         a.ctab = (const uint32_t *)c->ctab.p;
@@ -285,6 +293,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     a.wbest = (BestRec *)c->wbest.p;
     a.best = (BestRec *)c->best.p;
     a.err = (int32_t *)c->errf.p;
+    a.gbest = a.err + 2;
     a.srows = nullptr;
     a.sr_every = 1;
     a.nsr = 0;
@@ -292,7 +301,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     c->last_nstrips = plan.nstrips;
     if (c->opts.verbose & 2) {  // stage-1 strip trace, read back with swb_trace_copy
         if ((e = c->trace.ensure(sizeof(int64_t) * 3 * (size_t)plan.nstrips)) != cudaSuccess)
-            return cuda_fail(c, e, "trace buffer");
+            return ctx_cuda_fail(c, e, "trace buffer");
         a.trace = (int64_t *)c->trace.p;
     }
     a.scols = nullptr;
@@ -317,16 +326,16 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
         }
     }
     if (sbytes > c->opts.hbm_budget_bytes)
-        return fail(c, SWB_ENOMEM_BUDGET, "special rows and columns need %zu bytes > budget %llu", sbytes,
+        return ctx_fail(c, SWB_ENOMEM_BUDGET, "special rows and columns need %zu bytes > budget %llu", sbytes,
                     (unsigned long long)c->opts.hbm_budget_bytes);
     if (a.nsr > 0) {
         if ((e = c->srows.ensure(sizeof(int2) * (size_t)a.nsr * (size_t)n)) != cudaSuccess)
-            return cuda_fail(c, e, "special rows");
+            return ctx_cuda_fail(c, e, "special rows");
         a.srows = (int2 *)c->srows.p;
     }
     if (a.nsc > 0) {
         if ((e = c->scols.ensure(sizeof(int2) * (size_t)a.nsc * (size_t)m)) != cudaSuccess)
-            return cuda_fail(c, e, "special columns");
+            return ctx_cuda_fail(c, e, "special columns");
         a.scols = (int2 *)c->scols.p;
     }
     c->last_nsr = a.nsr;
@@ -343,16 +352,16 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
 
     if ((e = cudaMemsetAsync(a.hbuf, 0xFF, sizeof(int4) * (size_t)n, c->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(a.err, 0, 4 * sizeof(int32_t), c->stream)) != cudaSuccess)
-        return cuda_fail(c, e, "stage 1 reset");
+        return ctx_cuda_fail(c, e, "stage 1 reset");
     cudaEventRecord(c->ev0, c->stream);
-    if ((e = stage1_launch(a, plan, c->stream)) != cudaSuccess) return cuda_fail(c, e, "stage 1 launch");
+    if ((e = stage1_launch(a, plan, c->stream)) != cudaSuccess) return ctx_cuda_fail(c, e, "stage 1 launch");
     cudaEventRecord(c->ev1, c->stream);
     int32_t errh[2] = {0, 0};
     if ((e = cudaMemcpyAsync(best_out, a.best, sizeof(BestRec), cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
         (e = cudaMemcpyAsync(errh, a.err, sizeof errh, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
-        return cuda_fail(c, e, "stage 1");
-    if (errh[0] != 0) return fail(c, SWB_ETIMEOUT, "stage 1: a bounded wait between strips ran out");
+        return ctx_cuda_fail(c, e, "stage 1");
+    if (errh[0] != 0) return ctx_fail(c, SWB_ETIMEOUT, "stage 1: a bounded wait between strips ran out");
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     if (ms_out) *ms_out = ms;
@@ -416,7 +425,7 @@ int align_device(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_
         int32_t launches = 0;
         rc = tb::traceback(c->stream, c->sms, d_rows, m, d_cols, n, sc, plan, (const int2 *)c->srows.p,
                            (const int2 *)c->scols.p, out, scr, c->err, &launches);
-        if (rc != SWB_OK) return fail(c, rc, "%s", c->err.c_str());
+        if (rc != SWB_OK) return ctx_fail(c, rc, "%s", c->err.c_str());
         out->kernel_launches += launches;
         out->stage2_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
     } else if (!score_only) {
@@ -436,9 +445,9 @@ int align_device(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_
 extern "C" int swb_align_pair_device(swb_ctx *c, const void *d_rows, int64_t rows, const void *d_cols, int64_t cols,
                                      const swb_scoring *sc, uint32_t flags, swb_result *out) {
     if (!c || !out || rows < 0 || cols < 0 || rows < cols || (rows > 0 && !d_rows) || (cols > 0 && !d_cols))
-        return fail(c, SWB_EINVAL, "swb_align_pair_device: bad arguments");
+        return ctx_fail(c, SWB_EINVAL, "swb_align_pair_device: bad arguments");
     if (rows > (int64_t)INT32_MAX - 64 || cols > (int64_t)INT32_MAX - 64)
-        return fail(c, SWB_EUNSUPPORTED, "sequence longer than 2^31 - 64");
+        return ctx_fail(c, SWB_EUNSUPPORTED, "sequence longer than 2^31 - 64");
     int rc = check_scoring(c, sc, rows, cols);
     if (rc != SWB_OK) return rc;
     std::lock_guard<std::mutex> lk(c->mu);
@@ -449,48 +458,48 @@ extern "C" int swb_align_pair_device(swb_ctx *c, const void *d_rows, int64_t row
 extern "C" int swb_align_pair(swb_ctx *c, const uint8_t *a, int64_t la, const uint8_t *b, int64_t lb,
                               const swb_scoring *sc, uint32_t flags, swb_result *out) {
     if (!c || !out || la < 0 || lb < 0 || (la > 0 && !a) || (lb > 0 && !b))
-        return fail(c, SWB_EINVAL, "swb_align_pair: bad arguments");
+        return ctx_fail(c, SWB_EINVAL, "swb_align_pair: bad arguments");
     const bool swap = la < lb;  // src/SWutils.cpp:84-88
     const uint8_t *hr = swap ? b : a;
     const uint8_t *hc = swap ? a : b;
     const int64_t m = swap ? lb : la, n = swap ? la : lb;
     if (m > (int64_t)INT32_MAX - 64)
-        return fail(c, SWB_EUNSUPPORTED, "sequence longer than 2^31 - 64");
+        return ctx_fail(c, SWB_EUNSUPPORTED, "sequence longer than 2^31 - 64");
     int rc = check_scoring(c, sc, m, n);
     if (rc != SWB_OK) return rc;
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
     cudaError_t e;
     if ((e = c->rows.ensure((size_t)m + 64)) != cudaSuccess || (e = c->cols.ensure((size_t)n + 64)) != cudaSuccess)
-        return cuda_fail(c, e, "sequence buffers");
+        return ctx_cuda_fail(c, e, "sequence buffers");
     if (m > 0 && (e = cudaMemcpyAsync(c->rows.p, hr, (size_t)m, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
-        return cuda_fail(c, e, "copy rows");
+        return ctx_cuda_fail(c, e, "copy rows");
     if (n > 0 && (e = cudaMemcpyAsync(c->cols.p, hc, (size_t)n, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
-        return cuda_fail(c, e, "copy cols");
+        return ctx_cuda_fail(c, e, "copy cols");
     return align_device(c, (const uint8_t *)c->rows.p, m, (const uint8_t *)c->cols.p, n, sc, flags, out, swap ? 1 : 0);
 }
 
 // Copies special row `idx` (row (idx+1)*interval - 1) of the last call as (H, F)
 // pairs into host memory `out` (2*cols int32).  Inspection entry for tests.
 extern "C" int swb_special_row_copy(swb_ctx *c, int64_t idx, int32_t *out, int64_t cols, int64_t *interval) {
-    if (!c || !out) return fail(c, SWB_EINVAL, "swb_special_row_copy: bad arguments");
+    if (!c || !out) return ctx_fail(c, SWB_EINVAL, "swb_special_row_copy: bad arguments");
     if (interval) *interval = c->last_sr_interval;
     if (idx < 0 || idx >= c->last_nsr || cols != c->last_n)
-        return fail(c, SWB_EINVAL, "special row %lld not available", (long long)idx);
+        return ctx_fail(c, SWB_EINVAL, "special row %lld not available", (long long)idx);
     cudaSetDevice(c->device);
     cudaError_t e = cudaMemcpy(out, (const int2 *)c->srows.p + idx * c->last_n, sizeof(int2) * (size_t)cols,
                                cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return cuda_fail(c, e, "special row copy");
+    if (e != cudaSuccess) return ctx_cuda_fail(c, e, "special row copy");
     return SWB_OK;
 }
 
 // Copies the stage-1 strip trace of the last call (options.verbose bit 1 set):
 // per strip {start ns, end ns, SM id}.  Returns the number of strips in *count.
 extern "C" int swb_trace_copy(swb_ctx *c, int64_t *out, int64_t cap, int64_t *count) {
-    if (!c || !out || !count) return fail(c, SWB_EINVAL, "swb_trace_copy: bad arguments");
+    if (!c || !out || !count) return ctx_fail(c, SWB_EINVAL, "swb_trace_copy: bad arguments");
     *count = c->last_nstrips;
-    if (!c->trace.p || cap < 3 * c->last_nstrips) return fail(c, SWB_EINVAL, "no trace or buffer too small");
+    if (!c->trace.p || cap < 3 * c->last_nstrips) return ctx_fail(c, SWB_EINVAL, "no trace or buffer too small");
     cudaSetDevice(c->device);
     cudaError_t e = cudaMemcpy(out, c->trace.p, sizeof(int64_t) * 3 * (size_t)c->last_nstrips, cudaMemcpyDeviceToHost);
-    return e == cudaSuccess ? SWB_OK : cuda_fail(c, e, "trace copy");
+    return e == cudaSuccess ? SWB_OK : ctx_cuda_fail(c, e, "trace copy");
 }

@@ -1,0 +1,236 @@
+// batch.cu -- the batched scoring wavefront: many independent pairs of uneven
+// length in one persistent launch fed from a device work queue.
+//
+// No counterpart in the reference, which aligns one pair per process
+// (src/main.cu:102-249); every pair's recurrence, tie rule and special rows are
+// the single-pair ones (stage1_core.cuh), so a pair scores exactly the same
+// alone or in a batch.
+//
+// Work units.  A pair with m rows has ceil(m / 512) strips of 512 rows (16 rows
+// per lane).  The host lists every strip of every pair as one work unit, pair
+// after pair (longest pairs first, each pair's strips in order), and warps claim
+// units from a device counter.  A unit's only dependency is the strip above it,
+// which was claimed earlier by a warp that is resident (the launch is
+// cooperative), so every wait ends.  A short pair (<= 512 rows) is one unit: one
+// warp aligns it alone (inter-sequence mapping).  A longer pair's strips run on
+// consecutive warps that pass the strip's bottom row down through the pair's
+// tagged row buffer as in the single-pair kernel (intra-sequence wavefront).
+//
+// Each unit records the best cell of its strip; a second kernel merges the
+// strips of each pair (a warp per pair) into the pair's record, which may carry
+// the best of strips run by earlier launches (the serving loop runs a pair's
+// strips over several launches).
+#include <algorithm>
+#include <type_traits>
+
+#include "batch.h"
+#include "stage1_core.cuh"
+
+namespace swb {
+namespace {
+
+// Store fields of a pair view: none (score only) or per-pair special rows and
+// columns (store pass for the traceback).
+struct NoStores {
+    static constexpr int2 *srows = nullptr;
+    static constexpr int64_t sr_every = 1;
+    static constexpr int2 *scols = nullptr;
+    static constexpr int32_t sc_every = 1 << 30;
+};
+struct WithStores {
+    int2 *srows;
+    int64_t sr_every;
+    int2 *scols;
+    int32_t sc_every;
+};
+
+// The argument view the wavefront core reads for one pair of a batch.
+template <class S>
+struct PairView : S {
+    int32_t open, ext, gx, mt1, mm1;
+    uint32_t tab_hi;
+    int32_t *err;                  // [0] error code, [1] abort flag
+    const uint8_t *rows, *cols, *rcode;
+    const uint32_t *ctab;
+    int64_t m, n;
+    int4 *hbuf;
+    int32_t *gbest;
+    TieGeom tie;
+    static constexpr const int2 *top = nullptr;
+    static constexpr const int2 *left = nullptr;
+    static constexpr int32_t corner = 0;
+    static constexpr int64_t r_origin = 0;
+    static constexpr int64_t c_origin = 0;
+    static constexpr int64_t *trace = nullptr;
+};
+
+template <bool TAB, class S>
+__global__ void __launch_bounds__(kWarps * 32, (std::is_same<S, NoStores>::value ? 4 : 3)) batch_kernel(BatchArgs g) {
+    __shared__ int4 ring_all[kWarps][kRing];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    int4 *ring = ring_all[wib];
+    for (;;) {
+        __syncwarp();
+        int32_t u = 0;
+        if (lane == 0) u = atomicAdd(&g.ctl[0], 1);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= g.nunits || ld_volatile(&g.ctl[2]) != 0) break;
+        const BatchPair d = g.pairs[g.unit_pair[u]];
+        PairView<S> v;
+        v.open = g.open;
+        v.ext = g.ext;
+        v.gx = g.gx;
+        v.mt1 = g.mt1;
+        v.mm1 = g.mm1;
+        v.tab_hi = g.tab_hi;
+        v.err = g.ctl + 1;
+        v.rows = g.seq + d.row_off;
+        v.cols = g.seq + d.col_off;
+        v.rcode = TAB ? g.rcode + d.row_off : nullptr;
+        v.ctab = TAB ? g.ctab + d.col_off : nullptr;
+        v.m = d.m;
+        v.n = d.n;
+        v.hbuf = g.hbuf + d.hbuf_off;
+        v.gbest = g.gbest + d.slot;
+        v.tie = d.tie;
+        if constexpr (!std::is_same<S, NoStores>::value) {
+            v.srows = g.srows + d.sr_off;
+            v.sr_every = d.sr_every;
+            v.scols = g.scols + d.sc_off;
+            v.sc_every = d.sc_every;
+        }
+        Best b;
+        b.ho = g.open + 1;  // only H >= 1 is recorded
+        b.key = ~0ULL;
+        b.row = 0;
+        b.col = 0;
+        int32_t bho = b.ho;
+        if (!run_strip<kBatchR, TAB>(v, ring, lane, u - d.unit0, &b, bho)) {
+            if (lane == 0) {
+                atomicCAS(&g.ctl[1], kErrNone, kErrTimeout);
+                atomicExch(&g.ctl[2], 1);
+            }
+            break;
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const int32_t oho = __shfl_xor_sync(0xffffffffu, b.ho, off);
+            const uint64_t okey = __shfl_xor_sync(0xffffffffu, b.key, off);
+            const int64_t orow = __shfl_xor_sync(0xffffffffu, b.row, off);
+            const int64_t ocol = __shfl_xor_sync(0xffffffffu, b.col, off);
+            if (better(oho, okey, b.ho, b.key)) {
+                b.ho = oho;
+                b.key = okey;
+                b.row = orow;
+                b.col = ocol;
+            }
+        }
+        if (lane == 0) {
+            BestRec r;
+            r.ho = b.ho;
+            r.valid = (b.key != ~0ULL) ? 1 : 0;
+            r.key = b.key;
+            r.row = b.row;
+            r.col = b.col;
+            g.ubest[u] = r;
+        }
+    }
+}
+
+__device__ __forceinline__ void merge(BestRec &b, const BestRec &r) {
+    if (r.valid && (!b.valid || better(r.ho, r.key, b.ho, b.key))) b = r;
+}
+
+// A warp per pair: merges the pair's units of this launch into pbest[slot].
+__global__ void batch_reduce_kernel(const BatchPair *pairs, int64_t npairs, const BestRec *ubest, BestRec *pbest) {
+    const int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (p >= npairs) return;
+    const BatchPair d = pairs[p];
+    BestRec b;
+    b.ho = INT_MIN;
+    b.valid = 0;
+    b.key = ~0ULL;
+    b.row = 0;
+    b.col = 0;
+    if (lane == 0) b = pbest[d.slot];
+    for (int32_t u = d.ufirst + lane; u < d.ufirst + d.ucount; u += 32) merge(b, ubest[u]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        BestRec o;
+        o.ho = __shfl_xor_sync(0xffffffffu, b.ho, off);
+        o.valid = __shfl_xor_sync(0xffffffffu, b.valid, off);
+        o.key = __shfl_xor_sync(0xffffffffu, b.key, off);
+        o.row = __shfl_xor_sync(0xffffffffu, b.row, off);
+        o.col = __shfl_xor_sync(0xffffffffu, b.col, off);
+        merge(b, o);
+    }
+    if (lane == 0) pbest[d.slot] = b;
+}
+
+__global__ void batch_encode_kernel(const uint8_t *seq, int64_t bytes, const uint8_t *lut, uint8_t *rcode,
+                                    uint32_t *ctab, uint32_t mm4, uint32_t x1) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < bytes; i += stride) {
+        const uint32_t q = lut[seq[i]];
+        rcode[i] = (uint8_t)q;
+        ctab[i] = q < 4 ? (mm4 ^ (x1 << (8 * q))) : mm4;
+    }
+}
+
+template <bool TAB, class S>
+int max_blocks() {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_kernel<TAB, S>, kWarps * 32, 0) != cudaSuccess)
+        return 0;
+    return nb;
+}
+
+template <bool TAB, class S>
+cudaError_t launch(const BatchArgs &a, int sms, cudaStream_t st) {
+    const int per_sm = std::max(1, max_blocks<TAB, S>());
+    const int64_t need = (a.nunits + kWarps - 1) / kWarps;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)per_sm * sms));
+    BatchArgs copy = a;
+    void *args[] = {&copy};
+    return cudaLaunchCooperativeKernel((const void *)batch_kernel<TAB, S>, dim3(blocks), dim3(kWarps * 32), args, 0,
+                                       st);
+}
+
+}  // namespace
+
+int batch_max_blocks_per_sm(bool tab, bool stores) {
+    if (stores) return tab ? max_blocks<true, WithStores>() : max_blocks<false, WithStores>();
+    return tab ? max_blocks<true, NoStores>() : max_blocks<false, NoStores>();
+}
+
+cudaError_t batch_launch(const BatchArgs &a, bool tab, bool stores, int sms, int64_t npairs, BestRec *pbest,
+                         cudaStream_t st) {
+    cudaError_t e = cudaSuccess;
+    if (a.nunits > 0) {
+        if (stores) e = tab ? launch<true, WithStores>(a, sms, st) : launch<false, WithStores>(a, sms, st);
+        else e = tab ? launch<true, NoStores>(a, sms, st) : launch<false, NoStores>(a, sms, st);
+        if (e != cudaSuccess) return e;
+    }
+    if (npairs > 0) {
+        const int64_t threads = npairs * 32;
+        batch_reduce_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(a.pairs, npairs, a.ubest, pbest);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+cudaError_t batch_encode(const uint8_t *seq, int64_t bytes, const uint8_t *d_lut, uint8_t *rcode, uint32_t *ctab,
+                         int32_t mt1, int32_t mm1, uint32_t *tab_hi, cudaStream_t st) {
+    const uint32_t mmb = (uint32_t)(uint8_t)(int8_t)mm1;
+    const uint32_t mm4 = mmb * 0x01010101u;
+    const uint32_t x1 = ((uint32_t)(uint8_t)(int8_t)mt1 ^ mmb) & 0xFFu;
+    *tab_hi = mm4;
+    if (bytes <= 0) return cudaSuccess;
+    const int blocks = (int)std::min<int64_t>(8192, (bytes + 255) / 256);
+    batch_encode_kernel<<<blocks, 256, 0, st>>>(seq, bytes, d_lut, rcode, ctab, mm4, x1);
+    return cudaGetLastError();
+}
+
+}  // namespace swb

@@ -1,0 +1,63 @@
+// batch.h -- internal declarations of the batched wavefront (batch.cu), used by
+// the batched entry points (batch_host.cpp) and the serving loop (serve.cpp).
+#pragma once
+
+#include <cstdint>
+
+#include "swb_internal.h"
+
+namespace swb {
+
+// One pair of a batch on the device.  Rows are the longer sequence (m >= n >= 1).
+struct BatchPair {
+    int64_t row_off, col_off;  // byte offsets of rows / cols in the batch's sequence buffer
+    int64_t hbuf_off;          // first hbuf entry of the pair (n entries; pairs with one strip use none)
+    int64_t sr_off, sc_off;    // first special-row / special-column entry (store pass only)
+    int32_t m, n;
+    int32_t unit0;             // work unit u of this launch runs strip u - unit0 of the pair
+    int32_t nstrips;           // strips of the whole pair
+    int32_t slot;              // index of the pair's record in gbest / pbest
+    int32_t sc_every;          // store pass: a special column every sc_every columns (power of two)
+    int32_t sr_every;          // store pass: a special row every sr_every strips
+    int32_t ufirst, ucount;    // this launch's units of the pair: [ufirst, ufirst + ucount)
+    int32_t pad_;
+    TieGeom tie;               // tie rule of the pair (reference launch shape of its lengths)
+};
+
+// Uniform arguments of one batched launch.
+struct BatchArgs {
+    const uint8_t *seq;        // sequence bytes (CMP mode)
+    const uint8_t *rcode;      // TAB mode: per-byte code of seq
+    const uint32_t *ctab;      // TAB mode: per-byte table word of seq
+    int32_t open, ext, gx, mt1, mm1;
+    uint32_t tab_hi;
+    const BatchPair *pairs;
+    const int32_t *unit_pair;  // work unit -> index into pairs; units are claimed in this order
+    int64_t nunits;
+    int4 *hbuf;
+    int32_t *gbest;            // per pair slot: best H seen so far
+    BestRec *ubest;            // per work unit: best cell of that strip
+    int32_t *ctl;              // [0] unit counter, [1] error code, [2] abort flag
+    int2 *srows, *scols;       // store pass: special rows (H, F) / columns (H, E) of every pair
+};
+
+// Rows per lane of the batched kernel (its strips are 32 * kBatchR rows; the
+// store pass relies on 512-row strips for the walker's grid).
+constexpr int kBatchR = 16;
+constexpr int kBatchStripRows = 32 * kBatchR;
+
+// Launches the batched wavefront over units [0, a.nunits) (a.ctl must be zeroed
+// first), then merges the strips' best cells of pairs [0, npairs) of a.pairs
+// into pbest[slot] (which holds the pair's best so far, or an invalid record).
+// Every strip a launch runs must have its predecessor strip either earlier in the
+// same launch's unit order or finished by an earlier launch.  `stores` selects
+// the store pass.
+cudaError_t batch_launch(const BatchArgs &a, bool tab, bool stores, int sms, int64_t npairs, BestRec *pbest,
+                         cudaStream_t st);
+// Byte presence flags over a buffer (TAB-mode choice) and the TAB encodings of
+// every byte of seq (rcode[i] = lut[seq[i]], ctab[i] = table word of seq[i]).
+cudaError_t batch_encode(const uint8_t *seq, int64_t bytes, const uint8_t *d_lut, uint8_t *rcode, uint32_t *ctab,
+                         int32_t mt1, int32_t mm1, uint32_t *tab_hi, cudaStream_t st);
+int batch_max_blocks_per_sm(bool tab, bool stores);
+
+}  // namespace swb

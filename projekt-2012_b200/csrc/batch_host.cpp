@@ -1,0 +1,440 @@
+// batch_host.cpp -- the batched entry points (swb_batch_align*): orientation,
+// work-unit layout, the scoring launch, and for the best-scoring pairs a store
+// pass plus the batched walker.  No counterpart in the reference (one pair per
+// process, src/main.cu:102-249).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "batch.h"
+#include "ctx.h"
+#include "traceback.h"
+
+namespace swb {
+namespace {
+
+struct PairInfo {
+    int64_t row_off, col_off;
+    int64_t m, n;
+    int32_t swapped;
+};
+
+// Lays out the units of `order` (indices into info, already sorted) as one
+// launch: unit0 / ufirst / ucount / hbuf offsets; returns the unit count.
+int64_t layout_units(const std::vector<PairInfo> &info, const std::vector<int64_t> &order, uint32_t flags,
+                     std::vector<BatchPair> &bp, std::vector<int32_t> &unit_pair, int64_t *hbuf_entries) {
+    bp.resize(order.size());
+    unit_pair.clear();
+    int64_t units = 0, hb = 0;
+    for (size_t k = 0; k < order.size(); ++k) {
+        const PairInfo &p = info[(size_t)order[k]];
+        BatchPair &d = bp[k];
+        std::memset(&d, 0, sizeof d);
+        d.row_off = p.row_off;
+        d.col_off = p.col_off;
+        d.m = (int32_t)p.m;
+        d.n = (int32_t)p.n;
+        d.nstrips = (int32_t)((p.m + kBatchStripRows - 1) / kBatchStripRows);
+        d.unit0 = (int32_t)units;
+        d.ufirst = (int32_t)units;
+        d.ucount = d.nstrips;
+        d.slot = (int32_t)k;
+        d.sr_every = 1;
+        d.sc_every = 1 << 30;
+        if (d.nstrips > 1) {
+            d.hbuf_off = hb;
+            hb += p.n;
+        }
+        int32_t G = 0, T = 0;
+        int64_t P1 = 0, P2 = 0;
+        const bool refok = reference_geometry(p.m, p.n, &G, &T, &P1, &P2);
+        d.tie.mode = ((flags & SWB_FLAG_TIE_ROWMAJOR) || !refok) ? kTieRowMajor : kTieReference;
+        d.tie.G = G;
+        d.tie.T = T;
+        d.tie.C = refok ? P2 / G : 1;
+        for (int32_t s = 0; s < d.nstrips; ++s) unit_pair.push_back((int32_t)k);
+        units += d.nstrips;
+    }
+    *hbuf_entries = hb;
+    return units;
+}
+
+// Runs one scoring launch (optionally the store pass) over bp; pbest receives
+// one record per entry of bp (slot k).
+int run_launch(swb_ctx *c, const uint8_t *d_seq, bool tab, const BatchArgs &base, std::vector<BatchPair> &bp,
+               std::vector<int32_t> &unit_pair, int64_t hbuf_entries, bool stores, std::vector<BestRec> &pbest,
+               float *ms) {
+    cudaError_t e;
+    const int64_t np = (int64_t)bp.size(), nu = (int64_t)unit_pair.size();
+    const size_t bp_bytes = sizeof(BatchPair) * (size_t)np, up_bytes = sizeof(int32_t) * (size_t)nu;
+    if ((e = c->b_pairs.ensure(bp_bytes)) != cudaSuccess || (e = c->b_units.ensure(up_bytes)) != cudaSuccess ||
+        (e = c->b_hbuf.ensure(sizeof(int4) * (size_t)std::max<int64_t>(1, hbuf_entries))) != cudaSuccess ||
+        (e = c->b_gbest.ensure(sizeof(int32_t) * (size_t)np)) != cudaSuccess ||
+        (e = c->b_ubest.ensure(sizeof(BestRec) * (size_t)std::max<int64_t>(1, nu))) != cudaSuccess ||
+        (e = c->b_pbest.ensure(sizeof(BestRec) * (size_t)np)) != cudaSuccess ||
+        (e = c->b_ctl.ensure(4 * sizeof(int32_t))) != cudaSuccess ||
+        (e = c->h_stage.ensure(std::max(bp_bytes + up_bytes, sizeof(BestRec) * (size_t)np) + 64)) != cudaSuccess)
+        return ctx_cuda_fail(c, e, "batch buffers");
+    // descriptors through pinned staging (one buffer, two copies)
+    uint8_t *hs = (uint8_t *)c->h_stage.p;
+    std::memcpy(hs, bp.data(), bp_bytes);
+    std::memcpy(hs + bp_bytes, unit_pair.data(), up_bytes);
+    BatchArgs a = base;
+    a.seq = d_seq;
+    a.pairs = (const BatchPair *)c->b_pairs.p;
+    a.unit_pair = (const int32_t *)c->b_units.p;
+    a.nunits = nu;
+    a.hbuf = (int4 *)c->b_hbuf.p;
+    a.gbest = (int32_t *)c->b_gbest.p;
+    a.ubest = (BestRec *)c->b_ubest.p;
+    a.ctl = (int32_t *)c->b_ctl.p;
+    if ((e = cudaMemcpyAsync(c->b_pairs.p, hs, bp_bytes, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(c->b_units.p, hs + bp_bytes, up_bytes, cudaMemcpyHostToDevice, c->stream)) !=
+            cudaSuccess ||
+        (hbuf_entries > 0 &&
+         (e = cudaMemsetAsync(a.hbuf, 0xFF, sizeof(int4) * (size_t)hbuf_entries, c->stream)) != cudaSuccess) ||
+        (e = cudaMemsetAsync(a.gbest, 0, sizeof(int32_t) * (size_t)np, c->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(c->b_pbest.p, 0, sizeof(BestRec) * (size_t)np, c->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(a.ctl, 0, 4 * sizeof(int32_t), c->stream)) != cudaSuccess)
+        return ctx_cuda_fail(c, e, "batch set-up");
+    cudaEventRecord(c->ev0, c->stream);
+    if ((e = batch_launch(a, tab, stores, c->sms, np, (BestRec *)c->b_pbest.p, c->stream)) != cudaSuccess)
+        return ctx_cuda_fail(c, e, "batch launch");
+    cudaEventRecord(c->ev1, c->stream);
+    int32_t ctl[4] = {0, 0, 0, 0};
+    pbest.resize((size_t)np);
+    if ((e = cudaMemcpyAsync(hs, c->b_pbest.p, sizeof(BestRec) * (size_t)np, cudaMemcpyDeviceToHost, c->stream)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(ctl, a.ctl, sizeof ctl, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+        return ctx_cuda_fail(c, e, "batch");
+    if (ctl[1] != 0) return ctx_fail(c, SWB_ETIMEOUT, "batch: a bounded wait between strips ran out");
+    std::memcpy(pbest.data(), hs, sizeof(BestRec) * (size_t)np);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, c->ev0, c->ev1);
+    if (ms) *ms += t;
+    return SWB_OK;
+}
+
+int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t seq_bytes, const swb_pair_ref *pairs,
+              int64_t npairs, const swb_scoring *sc, uint32_t flags, double trace_frac, swb_batch_result *out) {
+    const auto t0 = std::chrono::steady_clock::now();
+    std::memset(out, 0, sizeof *out);
+    if (!sc) return ctx_fail(c, SWB_EINVAL, "scoring is NULL");
+    if (sc->match < 1 || sc->mismatch > -1 || sc->gap_open > -1 || sc->gap_extend > -1)
+        return ctx_fail(c, SWB_EINVAL, "One or more scoring values were not usable!");
+    if (npairs < 0 || (npairs > 0 && !pairs) || seq_bytes < 0 || !(trace_frac >= 0.0 && trace_frac <= 1.0))
+        return ctx_fail(c, SWB_EINVAL, "swb_batch_align: bad arguments");
+    if (npairs > (int64_t)INT32_MAX / 4) return ctx_fail(c, SWB_EUNSUPPORTED, "too many pairs in one batch");
+    // orientation of every pair (src/SWutils.cpp:84-88: the longer one is rows)
+    std::vector<PairInfo> info((size_t)npairs);
+    int64_t maxlen = 0, cells = 0;
+    for (int64_t i = 0; i < npairs; ++i) {
+        const swb_pair_ref &r = pairs[i];
+        if (r.a_off < 0 || r.a_len < 0 || r.b_off < 0 || r.b_len < 0 || r.a_off > seq_bytes ||
+            r.a_len > seq_bytes - r.a_off || r.b_off > seq_bytes || r.b_len > seq_bytes - r.b_off)
+            return ctx_fail(c, SWB_EINVAL, "pair %lld: byte range outside the sequence buffer", (long long)i);
+        PairInfo &p = info[(size_t)i];
+        p.swapped = r.a_len < r.b_len ? 1 : 0;
+        p.row_off = p.swapped ? r.b_off : r.a_off;
+        p.col_off = p.swapped ? r.a_off : r.b_off;
+        p.m = std::max(r.a_len, r.b_len);
+        p.n = std::min(r.a_len, r.b_len);
+        if (p.m > (int64_t)INT32_MAX - 64) return ctx_fail(c, SWB_EUNSUPPORTED, "sequence longer than 2^31 - 64");
+        maxlen = std::max(maxlen, p.m + p.n);
+        cells += p.m * p.n;
+    }
+    {
+        const long double worst = (long double)std::max(std::max(sc->match, -sc->mismatch),
+                                                        std::max(-sc->gap_open, -sc->gap_extend)) *
+                                  (long double)(maxlen + 2);
+        if (worst > 2.0e9L) return ctx_fail(c, SWB_EUNSUPPORTED, "scores would leave the int32 range");
+    }
+    out->npairs = npairs;
+    out->cells = cells;
+    out->items = (swb_batch_item *)std::calloc((size_t)std::max<int64_t>(1, npairs), sizeof(swb_batch_item));
+    if (!out->items) return ctx_fail(c, SWB_ENOMEM, "out of host memory");
+    for (int64_t i = 0; i < npairs; ++i) out->items[i].swapped = info[(size_t)i].swapped;
+
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    cudaError_t e;
+    const uint8_t *d_seq = d_seq_in;
+    if (h_seq) {
+        if ((e = c->b_seq.ensure((size_t)seq_bytes + 64)) != cudaSuccess) return ctx_cuda_fail(c, e, "batch sequences");
+        if (seq_bytes > 0 &&
+            (e = cudaMemcpyAsync(c->b_seq.p, h_seq, (size_t)seq_bytes, cudaMemcpyHostToDevice, c->stream)) !=
+                cudaSuccess)
+            return ctx_cuda_fail(c, e, "copy batch sequences");
+        d_seq = (const uint8_t *)c->b_seq.p;
+    }
+    // active pairs (both sequences non-empty), longest first (ties: lower index)
+    std::vector<int64_t> order;
+    order.reserve((size_t)npairs);
+    for (int64_t i = 0; i < npairs; ++i)
+        if (info[(size_t)i].n > 0) order.push_back(i);
+    std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
+        return info[(size_t)x].m * info[(size_t)x].n > info[(size_t)y].m * info[(size_t)y].n;
+    });
+
+    BatchArgs base{};
+    base.open = sc->gap_open;
+    base.ext = sc->gap_extend;
+    base.gx = std::max(sc->gap_open, sc->gap_extend);
+    base.mt1 = sc->match - sc->gap_open;
+    base.mm1 = sc->mismatch - sc->gap_open;
+    bool tab = false;
+    int32_t launches = 0;
+    if (!order.empty() && base.mt1 >= -128 && base.mt1 <= 127 && base.mm1 >= -128 && base.mm1 <= 127) {
+        // TAB mode when the whole buffer holds at most four distinct bytes
+        uint32_t present[256];
+        if ((e = c->flags.ensure(256 * sizeof(uint32_t))) != cudaSuccess ||
+            (e = stage1_presence(d_seq, seq_bytes, (uint32_t *)c->flags.p, c->stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(present, c->flags.p, sizeof present, cudaMemcpyDeviceToHost, c->stream)) !=
+                cudaSuccess ||
+            (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+            return ctx_cuda_fail(c, e, "batch alphabet");
+        launches += 1;
+        uint8_t lut[256];
+        int K = 0;
+        for (int i = 0; i < 256; ++i) lut[i] = present[i] ? (uint8_t)(K++) : 7;
+        if (K <= 4) {
+            tab = true;
+            if ((e = c->lut.ensure(256)) != cudaSuccess || (e = c->b_rcode.ensure((size_t)seq_bytes + 64)) != cudaSuccess ||
+                (e = c->b_ctab.ensure(sizeof(uint32_t) * ((size_t)seq_bytes + 64))) != cudaSuccess ||
+                (e = cudaMemcpyAsync(c->lut.p, lut, 256, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+                (e = batch_encode(d_seq, seq_bytes, (const uint8_t *)c->lut.p, (uint8_t *)c->b_rcode.p,
+                                  (uint32_t *)c->b_ctab.p, base.mt1, base.mm1, &base.tab_hi, c->stream)) != cudaSuccess)
+                return ctx_cuda_fail(c, e, "batch encode");
+            launches += 1;
+            base.rcode = (const uint8_t *)c->b_rcode.p;
+            base.ctab = (const uint32_t *)c->b_ctab.p;
+        }
+    }
+
+    // scoring launch
+    std::vector<BatchPair> bp;
+    std::vector<int32_t> unit_pair;
+    std::vector<BestRec> pbest;
+    int64_t hb = 0;
+    float ms1 = 0.f;
+    layout_units(info, order, flags, bp, unit_pair, &hb);
+    if (!order.empty()) {
+        int rc = run_launch(c, d_seq, tab, base, bp, unit_pair, hb, false, pbest, &ms1);
+        if (rc != SWB_OK) return rc;
+        launches += 2;
+    }
+    for (size_t k = 0; k < order.size(); ++k) {
+        swb_batch_item &it = out->items[order[k]];
+        const BestRec &b = pbest[k];
+        if (b.valid) {
+            it.score = b.ho - sc->gap_open;
+            it.end_row = b.row;
+            it.end_col = b.col;
+        }
+    }
+    for (int64_t i = 0; i < npairs; ++i) {
+        swb_batch_item &it = out->items[i];
+        it.start_row = it.end_row;
+        it.start_col = it.end_col;
+        int32_t G = 0, T = 0;
+        int64_t P1 = 0, P2 = 0;
+        reference_geometry(info[(size_t)i].m, info[(size_t)i].n, &G, &T, &P1, &P2);
+        it.xpoint_interval = T > 0 ? 4 * T : 20;
+    }
+    out->stage1_ms = ms1;
+
+    // traceback of the best-scoring pairs
+    const int64_t ntrace = std::min<int64_t>(npairs, (int64_t)std::ceil(trace_frac * (double)npairs - 1e-9));
+    if (ntrace > 0) {
+        const auto t1 = std::chrono::steady_clock::now();
+        std::vector<int64_t> byscore((size_t)npairs);
+        std::iota(byscore.begin(), byscore.end(), 0);
+        std::stable_sort(byscore.begin(), byscore.end(),
+                         [&](int64_t x, int64_t y) { return out->items[x].score > out->items[y].score; });
+        byscore.resize((size_t)ntrace);
+        std::sort(byscore.begin(), byscore.end());
+        std::vector<int64_t> tr;  // traced pairs that have an alignment (score > 0)
+        for (int64_t i : byscore) {
+            out->items[i].traced = 1;
+            if (out->items[i].score > 0) tr.push_back(i);
+        }
+        out->n_traced = ntrace;
+        // store pass over the traced pairs: special rows every 512 rows (every
+        // strip), special columns every 256 columns
+        const int kBC = tb::block_cols();
+        std::vector<BatchPair> bp2;
+        std::vector<int32_t> up2;
+        int64_t hb2 = 0;
+        layout_units(info, tr, flags, bp2, up2, &hb2);
+        int64_t srn = 0, scn = 0, ops_total = 0, xp_total = 0;
+        for (size_t k = 0; k < tr.size(); ++k) {
+            BatchPair &d = bp2[k];
+            d.sr_every = 1;
+            d.sc_every = kBC;
+            d.sr_off = srn;
+            d.sc_off = scn;
+            srn += (int64_t)(d.m / kBatchStripRows) * d.n;
+            scn += (int64_t)(d.n / kBC) * d.m;
+            ops_total += (int64_t)d.m + d.n + 8;
+            xp_total += d.m / out->items[tr[k]].xpoint_interval + 8;
+        }
+        if ((uint64_t)(srn + scn) * sizeof(int2) > c->opts.hbm_budget_bytes)
+            return ctx_fail(c, SWB_ENOMEM_BUDGET, "traced pairs' special rows and columns exceed the HBM budget");
+        const int kS = tb::state_slots();
+        if ((e = c->b_srows.ensure(sizeof(int2) * (size_t)std::max<int64_t>(1, srn))) != cudaSuccess ||
+            (e = c->b_scols.ensure(sizeof(int2) * (size_t)std::max<int64_t>(1, scn))) != cudaSuccess ||
+            (e = c->b_ops.ensure((size_t)std::max<int64_t>(1, ops_total))) != cudaSuccess ||
+            (e = c->b_xps.ensure(sizeof(int64_t) * 4 * (size_t)std::max<int64_t>(1, xp_total))) != cudaSuccess ||
+            (e = c->b_state.ensure(sizeof(int64_t) * kS * std::max<size_t>(1, tr.size()))) != cudaSuccess ||
+            (e = c->b_walk.ensure(tb::walk_args_bytes() * std::max<size_t>(1, tr.size()))) != cudaSuccess)
+            return ctx_cuda_fail(c, e, "batch traceback buffers");
+        float ms2 = 0.f;
+        if (!tr.empty()) {
+            BatchArgs b2 = base;
+            b2.srows = (int2 *)c->b_srows.p;
+            b2.scols = (int2 *)c->b_scols.p;
+            std::vector<BestRec> pb2;
+            int rc = run_launch(c, d_seq, tab, b2, bp2, up2, hb2, true, pb2, &ms2);
+            if (rc != SWB_OK) return rc;
+            launches += 2;
+            std::vector<tb::WalkInputs> win(tr.size());
+            std::vector<int64_t> st((size_t)kS * tr.size(), 0);
+            int64_t oo = 0, xo = 0;
+            std::vector<int64_t> ops_off(tr.size()), xp_off(tr.size());
+            for (size_t k = 0; k < tr.size(); ++k) {
+                const swb_batch_item &it = out->items[tr[k]];
+                const BatchPair &d = bp2[k];
+                const BestRec &b = pb2[k];
+                if (!b.valid || b.ho - sc->gap_open != it.score || b.row != it.end_row || b.col != it.end_col)
+                    return ctx_fail(c, SWB_ECUDA, "batch: store pass disagrees with the scoring pass");
+                tb::WalkInputs &w = win[k];
+                w.rows = d_seq + d.row_off;
+                w.cols = d_seq + d.col_off;
+                w.m = d.m;
+                w.n = d.n;
+                w.sc = *sc;
+                w.score = it.score;
+                w.srows = (const int2 *)c->b_srows.p + d.sr_off;
+                w.scols = (const int2 *)c->b_scols.p + d.sc_off;
+                w.rr0 = 0;
+                w.cc0 = 0;
+                w.rr1 = d.m;
+                w.cc1 = d.n;
+                w.rtop = nullptr;
+                w.rleft = nullptr;
+                w.rcorner = 0;
+                w.xp_interval = it.xpoint_interval;
+                w.ops = (char *)c->b_ops.p + oo;
+                w.ops_cap = (int64_t)d.m + d.n + 8;
+                w.xps = (int64_t *)c->b_xps.p + 4 * xo;
+                w.xp_cap = d.m / it.xpoint_interval + 8;
+                ops_off[k] = oo;
+                xp_off[k] = xo;
+                oo += w.ops_cap;
+                xo += w.xp_cap;
+                int64_t *S = st.data() + (size_t)kS * k;
+                S[tb::slot_r()] = it.end_row;
+                S[tb::slot_c()] = it.end_col;
+            }
+            std::string err;
+            rc = tb::walk_batch(c->stream, c->sms, win.data(), (int64_t)win.size(), c->b_walk.p,
+                                (int64_t *)c->b_state.p, st.data(), err);
+            if (rc != SWB_OK) return ctx_fail(c, rc, "%s", err.c_str());
+            launches += 1;
+            // gather: ops (end -> start on the device) and crosspoints
+            int64_t tot_ops = 0, tot_xp = 0;
+            for (size_t k = 0; k < tr.size(); ++k) {
+                const int64_t *S = st.data() + (size_t)kS * k;
+                if (S[tb::slot_nops()] > win[k].ops_cap || S[tb::slot_nxp()] > win[k].xp_cap)
+                    return ctx_fail(c, SWB_ECUDA, "batch traceback output larger than its buffers");
+                tot_ops += S[tb::slot_nops()];
+                tot_xp += S[tb::slot_nxp()] + 2;
+            }
+            std::vector<char> hops((size_t)std::max<int64_t>(1, oo));
+            std::vector<int64_t> hxp((size_t)std::max<int64_t>(4, 4 * xo));
+            if ((e = cudaMemcpyAsync(hops.data(), c->b_ops.p, (size_t)oo, cudaMemcpyDeviceToHost, c->stream)) !=
+                    cudaSuccess ||
+                (e = cudaMemcpyAsync(hxp.data(), c->b_xps.p, sizeof(int64_t) * 4 * (size_t)xo, cudaMemcpyDeviceToHost,
+                                     c->stream)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+                return ctx_cuda_fail(c, e, "batch traceback copy");
+            out->ops = (char *)std::malloc((size_t)tot_ops + 1);
+            out->xpoints = (swb_xpoint *)std::malloc(sizeof(swb_xpoint) * (size_t)(tot_xp + 2 * ntrace + 1));
+            if (!out->ops || !out->xpoints) return ctx_fail(c, SWB_ENOMEM, "out of host memory");
+            int64_t po = 0, px = 0;
+            for (size_t k = 0; k < tr.size(); ++k) {
+                swb_batch_item &it = out->items[tr[k]];
+                const int64_t *S = st.data() + (size_t)kS * k;
+                const int64_t nops = S[tb::slot_nops()], nxp = S[tb::slot_nxp()];
+                it.ops_off = po;
+                it.n_ops = nops;
+                std::reverse_copy(hops.data() + ops_off[k], hops.data() + ops_off[k] + nops, out->ops + po);
+                po += nops;
+                it.start_row = S[tb::slot_start_r()];
+                it.start_col = S[tb::slot_start_c()];
+                it.xp_off = px;
+                out->xpoints[px++] = swb_xpoint{0, 0, it.start_row, it.start_col};
+                for (int64_t q = nxp - 1; q >= 0; --q) {
+                    const int64_t *d = hxp.data() + 4 * (xp_off[k] + q);
+                    out->xpoints[px++] = swb_xpoint{(int32_t)d[3], (int32_t)d[2], d[0], d[1]};
+                }
+                out->xpoints[px++] = swb_xpoint{0, it.score, it.end_row, it.end_col};
+                it.n_xpoints = px - it.xp_off;
+            }
+            out->ops_bytes = po;
+            out->ops[po] = 0;
+            out->n_xpoints = px;
+        }
+        // traced pairs with score 0: no alignment; crosspoints [start = end]
+        for (int64_t i : byscore) {
+            swb_batch_item &it = out->items[i];
+            if (it.score > 0) continue;
+            if (!out->xpoints) {
+                out->xpoints = (swb_xpoint *)std::malloc(sizeof(swb_xpoint) * (size_t)(ntrace + 1));
+                if (!out->xpoints) return ctx_fail(c, SWB_ENOMEM, "out of host memory");
+            }
+            it.xp_off = out->n_xpoints;
+            it.n_xpoints = 1;
+            out->xpoints[out->n_xpoints++] = swb_xpoint{0, 0, it.end_row, it.end_col};
+        }
+        out->stage2_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
+    }
+    out->kernel_launches = launches;
+    out->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return SWB_OK;
+}
+
+}  // namespace
+}  // namespace swb
+
+extern "C" int swb_batch_align(swb_ctx *c, const uint8_t *seq, int64_t seq_bytes, const swb_pair_ref *pairs,
+                               int64_t npairs, const swb_scoring *sc, uint32_t flags, double trace_frac,
+                               swb_batch_result *out) {
+    if (!c || !out || (seq_bytes > 0 && !seq)) return swb::ctx_fail(c, SWB_EINVAL, "swb_batch_align: bad arguments");
+    int rc = swb::batch_run(c, seq, nullptr, seq_bytes, pairs, npairs, sc, flags, trace_frac, out);
+    if (rc != SWB_OK) swb_batch_result_free(out);
+    return rc;
+}
+
+extern "C" int swb_batch_align_device(swb_ctx *c, const void *d_seq, int64_t seq_bytes, const swb_pair_ref *pairs,
+                                      int64_t npairs, const swb_scoring *sc, uint32_t flags, double trace_frac,
+                                      swb_batch_result *out) {
+    if (!c || !out || (seq_bytes > 0 && !d_seq))
+        return swb::ctx_fail(c, SWB_EINVAL, "swb_batch_align_device: bad arguments");
+    int rc = swb::batch_run(c, nullptr, (const uint8_t *)d_seq, seq_bytes, pairs, npairs, sc, flags, trace_frac, out);
+    if (rc != SWB_OK) swb_batch_result_free(out);
+    return rc;
+}
+
+extern "C" void swb_batch_result_free(swb_batch_result *r) {
+    if (!r) return;
+    std::free(r->items);
+    std::free(r->ops);
+    std::free(r->xpoints);
+    std::memset(r, 0, sizeof *r);
+}

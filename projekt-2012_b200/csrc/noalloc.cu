@@ -121,6 +121,7 @@ extern "C" int swb_score_pair_noalloc(int32_t device, const void *d_rows, int64_
     a.wbest = (BestRec *)(base + kOffWbest);
     a.best = (BestRec *)(base + kOffBest);
     a.err = (int32_t *)(base + kOffErr);
+    a.gbest = a.err + 2;
     a.srows = nullptr;
     a.sr_every = 1;
     a.nsr = 0;

@@ -60,6 +60,7 @@ struct Stage1Args {
     BestRec *wbest;        // one per warp of the grid
     BestRec *best;         // final reduced record
     int32_t *err;          // [0] error code, [1] abort flag, [2] best H seen so far (device-wide)
+    int32_t *gbest;        // best H seen so far in this matrix (err + 2 for a single pair)
     int64_t *trace;        // optional: per strip {start ns, end ns, SM id} (globaltimer)
     TieGeom tie;
 };

@@ -118,6 +118,7 @@ int traceback(cudaStream_t st, int sms, const uint8_t *d_rows, int64_t m, const 
             a.wbest = wb;
             a.best = bb;
             a.err = ee;
+            a.gbest = a.err + 2;
             a.trace = nullptr;
             a.tie.mode = kTieRowMajor;
             cudaError_t e;

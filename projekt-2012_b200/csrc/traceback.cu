@@ -65,10 +65,6 @@ struct WalkArgs {
 // walker state slots
 enum { kStR = 0, kStC, kStState, kStNOps, kStSuffix, kStNXp, kStDone, kStErr, kStStartR, kStStartC, kStN };
 
-__device__ __forceinline__ int32_t sub_score(const WalkArgs &a, int64_t r, int64_t c) {
-    return a.rows[r] == a.cols[c] ? a.match : a.mismatch;
-}
-
 // H, E, F of the boundary cells around a block (region-relative fetches).
 __device__ __forceinline__ int2 top_hf(const WalkArgs &a, int64_t R0, int64_t c) {
     // (H, F) of row R0 - 1 at column c (c >= cc0 - 1 handled by callers)
@@ -89,9 +85,28 @@ __device__ __forceinline__ int2 left_he(const WalkArgs &a, int64_t C0, int64_t r
     return a.scols[q * (a.rr1 - a.rr0) + (r - a.rr0)];
 }
 
+// Block inputs staged in shared memory before a recompute, so that the step loop
+// and the walk touch no global memory: the top boundary (H, F) of row R0 - 1 at
+// columns C0 - 1 .. C1 (index j + 1), and the row / column bytes of the block.
+struct Stage {
+    int2 top[kBC + 1];
+    uint8_t rb[kBR];
+    uint8_t cb[kBC];
+};
+
+__device__ void stage_block(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0, int64_t C1, Stage *s) {
+    const int64_t w = C1 - C0 + 1, h = R1 - R0 + 1;
+    for (int64_t j = (int64_t)threadIdx.x - 1; j < w; j += blockDim.x) {
+        s->top[j + 1] = top_hf(a, R0, C0 + j);
+        if (j >= 0) s->cb[j] = a.cols[C0 + j];
+    }
+    for (int64_t i = threadIdx.x; i < h; i += blockDim.x) s->rb[i] = a.rows[R0 + i];
+}
+
 // Recomputes block rows [R0, R1] x cols [C0, C1] into dir (row-major, kBC wide).
+// Expects stage_block() to have filled `s` (and a barrier after it).
 __device__ void recompute(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0, int64_t C1, uint8_t *dir,
-                          int2 *xchg) {
+                          int2 (*xchg)[kThreads / 32], const Stage *s) {
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
     const int64_t w = C1 - C0 + 1;
@@ -105,7 +120,7 @@ __device__ void recompute(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0,
             const int2 v = left_he(a, C0, r);
             Hl[i] = v.x;
             El[i] = v.y;
-            ra[i] = a.rows[r];
+            ra[i] = s->rb[r - R0];
         } else {
             Hl[i] = 0;
             El[i] = 0;
@@ -114,7 +129,7 @@ __device__ void recompute(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0,
     }
     // H of the row above my first row at column C0 - 1
     int32_t hdiag0;
-    if (t == 0) hdiag0 = top_hf(a, R0, C0 - 1).x;
+    if (t == 0) hdiag0 = s->top[0].x;
     else hdiag0 = (r0 - 1 <= R1) ? left_he(a, C0, r0 - 1).x : 0;
     int32_t upH = 0, upF = 0;  // (H, F) from the row above at my current column
     int32_t prevUpH = hdiag0;  // H of the row above at the previous column
@@ -123,13 +138,13 @@ __device__ void recompute(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0,
         const int64_t j = k - t;  // my column offset
         const bool act = (j >= 0 && j < w && r0 <= R1);
         if (t == 0 && j >= 0 && j < w) {
-            const int2 tv = top_hf(a, R0, C0 + j);
+            const int2 tv = s->top[j + 1];
             upH = tv.x;
             upF = tv.y;
         }
         int32_t oH = 0, oF = 0;
         if (act) {
-            const uint8_t cb = a.cols[C0 + j];
+            const uint8_t cb = s->cb[j];
             int32_t hd = prevUpH;
             int32_t hu = upH, fu = upF;
 #pragma unroll
@@ -155,14 +170,17 @@ __device__ void recompute(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0,
             oF = fu;
         }
         prevUpH = upH;
-        // hand (H, F) of my last row to the thread below for the next step
+        // hand (H, F) of my last row to the thread below for the next step; the
+        // cross-warp slot alternates between two buffers so one barrier per step
+        // orders both the write of step k and the reuse of the slot at step k + 2
         const int32_t sH = __shfl_up_sync(0xffffffffu, oH, 1);
         const int32_t sF = __shfl_up_sync(0xffffffffu, oF, 1);
-        if (lane == 31) xchg[warp] = make_int2(oH, oF);
+        int2 *xb = xchg[k & 1];
+        if (lane == 31) xb[warp] = make_int2(oH, oF);
         __syncthreads();
         if (t > 0) {
             if (lane == 0) {
-                const int2 v = xchg[warp - 1];
+                const int2 v = xb[warp - 1];
                 upH = v.x;
                 upF = v.y;
             } else {
@@ -171,12 +189,11 @@ __device__ void recompute(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0,
             }
             if (j + 1 == 0) prevUpH = hdiag0;  // my first column: diagonal from the left boundary
         }
-        __syncthreads();
     }
 }
 
 // Warp 0 walks the path through the block [R0, R1] x [C0, C1].
-__device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const uint8_t *dir, int64_t *S) {
+__device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const uint8_t *dir, const Stage *sg, int64_t *S) {
     const int lane = threadIdx.x & 31;
     int64_t r = S[kStR], c = S[kStC];
     int32_t state = (int32_t)S[kStState];
@@ -193,7 +210,7 @@ __device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const uint8_t *d
             const uint32_t bal = __ballot_sync(0xffffffffu, ok);
             const int nrun = (bal == 0xffffffffu) ? 32 : __ffs(~bal) - 1;
             int32_t s = 0;
-            if (lane < nrun) s = sub_score(a, rr, cc);
+            if (lane < nrun) s = sg->rb[rr - R0] == sg->cb[cc - C0] ? a.match : a.mismatch;
             // inclusive prefix of s over lanes: suffix after lane i's cell
             int32_t ps = s;
 #pragma unroll
@@ -227,7 +244,7 @@ __device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const uint8_t *d
                 if (src == SRC_DIAG) {  // the start cell
                     if (lane == 0 && nops < a.ops_cap) a.ops[nops] = 'M';
                     nops += 1;
-                    suffix += sub_score(a, r, c);
+                    suffix += sg->rb[r - R0] == sg->cb[c - C0] ? a.match : a.mismatch;
                     S[kStStartR] = r;
                     S[kStStartC] = c;
                     done = true;
@@ -317,12 +334,9 @@ __device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const uint8_t *d
     }
 }
 
-// One CTA: block after block until the start is reached or the path leaves the
-// region [rr0, .) x [cc0, .).
-__global__ void __launch_bounds__(kThreads) walk_kernel(WalkArgs a) {
-    extern __shared__ uint8_t dir[];
-    __shared__ int2 xchg[kThreads / 32];
-    __shared__ int64_t S[kStN];
+// Block after block until the start is reached or the path leaves the region
+// [rr0, .) x [cc0, .); the state is read from and written back to a.st.
+__device__ void walk_body(const WalkArgs &a, uint8_t *dir, int2 (*xchg)[kThreads / 32], Stage *sg, int64_t *S) {
     if (threadIdx.x < kStN) S[threadIdx.x] = a.st[threadIdx.x];
     __syncthreads();
     for (int guard = 0; guard < (1 << 30); ++guard) {
@@ -330,20 +344,40 @@ __global__ void __launch_bounds__(kThreads) walk_kernel(WalkArgs a) {
         if (S[kStDone] || S[kStErr] || r < a.rr0 || c < a.cc0) break;
         const int64_t R0 = a.rr0 + ((r - a.rr0) / kBR) * kBR;
         const int64_t C0 = a.cc0 + ((c - a.cc0) / kBC) * kBC;
-        recompute(a, R0, r, C0, c, dir, xchg);
+        stage_block(a, R0, r, C0, c, sg);
         __syncthreads();
-        if (threadIdx.x < 32) walk(a, R0, C0, dir, S);
+        recompute(a, R0, r, C0, c, dir, xchg, sg);
+        __syncthreads();
+        if (threadIdx.x < 32) walk(a, R0, C0, dir, sg, S);
         __syncthreads();
     }
     if (threadIdx.x < kStN) a.st[threadIdx.x] = S[threadIdx.x];
 }
 
-struct DevMem {
-    void *p = nullptr;
-    ~DevMem() {
-        if (p) cudaFree(p);
+// One CTA walks one region.
+__global__ void __launch_bounds__(kThreads) walk_kernel(WalkArgs a) {
+    extern __shared__ uint8_t dir[];
+    __shared__ int2 xchg[2][kThreads / 32];
+    __shared__ Stage sg;
+    __shared__ int64_t S[kStN];
+    walk_body(a, dir, xchg, &sg, S);
+}
+
+// Batched pairs: CTA b walks pairs b, b + gridDim.x, ... (each pair's whole
+// matrix is its region).
+__global__ void __launch_bounds__(kThreads) walk_batch_kernel(const WalkArgs *args, int64_t n) {
+    extern __shared__ uint8_t dir[];
+    __shared__ int2 xchg[2][kThreads / 32];
+    __shared__ Stage sg;
+    __shared__ int64_t S[kStN];
+    __shared__ WalkArgs sa;
+    for (int64_t p = blockIdx.x; p < n; p += gridDim.x) {
+        __syncthreads();
+        if (threadIdx.x == 0) sa = args[p];
+        __syncthreads();
+        walk_body(sa, dir, xchg, &sg, S);
     }
-};
+}
 
 }  // namespace
 
@@ -374,7 +408,7 @@ Plan plan_for(const swb_options &opts, int64_t m, int64_t n) {
     return p;
 }
 
-int walk_region(cudaStream_t st, const WalkInputs &in, int64_t *host_state, std::string &err) {
+static WalkArgs to_args(const WalkInputs &in) {
     WalkArgs a{};
     a.rows = in.rows;
     a.cols = in.cols;
@@ -400,16 +434,18 @@ int walk_region(cudaStream_t st, const WalkInputs &in, int64_t *host_state, std:
     a.xps = in.xps;
     a.xp_cap = in.xp_cap;
     a.st = in.dstate;
+    return a;
+}
+
+int walk_region(cudaStream_t st, const WalkInputs &in, int64_t *host_state, std::string &err) {
+    const WalkArgs a = to_args(in);
     cudaError_t e;
     const size_t smem = (size_t)kBR * kBC;
-    static bool attr_set = false;
-    if (!attr_set) {
-        if ((e = cudaFuncSetAttribute(walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
-            cudaSuccess) {
-            err = std::string("walker attribute: ") + cudaGetErrorString(e);
-            return SWB_ECUDA;
-        }
-        attr_set = true;
+    // the attribute is per device: set it on every call (cheap)
+    if ((e = cudaFuncSetAttribute(walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+        cudaSuccess) {
+        err = std::string("walker attribute: ") + cudaGetErrorString(e);
+        return SWB_ECUDA;
     }
     if ((e = cudaMemcpyAsync(in.dstate, host_state, sizeof(int64_t) * kStN, cudaMemcpyHostToDevice, st)) !=
         cudaSuccess) {
@@ -430,6 +466,44 @@ int walk_region(cudaStream_t st, const WalkInputs &in, int64_t *host_state, std:
     }
     return SWB_OK;
 }
+
+int walk_batch(cudaStream_t st, int sms, const WalkInputs *in, int64_t n, void *d_args, int64_t *d_states,
+               int64_t *host_states, std::string &err) {
+    if (n <= 0) return SWB_OK;
+    std::vector<WalkArgs> args((size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+        args[(size_t)i] = to_args(in[i]);
+        args[(size_t)i].st = d_states + i * kStN;
+    }
+    cudaError_t e;
+    const size_t smem = (size_t)kBR * kBC;
+    const int64_t grid = std::min<int64_t>(n, (int64_t)std::max(1, sms));
+    if ((e = cudaFuncSetAttribute(walk_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(d_args, args.data(), sizeof(WalkArgs) * (size_t)n, cudaMemcpyHostToDevice, st)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(d_states, host_states, sizeof(int64_t) * kStN * (size_t)n, cudaMemcpyHostToDevice,
+                             st)) != cudaSuccess) {
+        err = std::string("batched walker set-up: ") + cudaGetErrorString(e);
+        return SWB_ECUDA;
+    }
+    walk_batch_kernel<<<(unsigned)grid, kThreads, smem, st>>>((const WalkArgs *)d_args, n);
+    if ((e = cudaGetLastError()) != cudaSuccess ||
+        (e = cudaMemcpyAsync(host_states, d_states, sizeof(int64_t) * kStN * (size_t)n, cudaMemcpyDeviceToHost,
+                             st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+        err = std::string("batched walker: ") + cudaGetErrorString(e);
+        return SWB_ECUDA;
+    }
+    for (int64_t i = 0; i < n; ++i)
+        if (host_states[i * kStN + kStErr] || !host_states[i * kStN + kStDone]) {
+            err = "batched walker: inconsistent direction data";
+            return SWB_ECUDA;
+        }
+    return SWB_OK;
+}
+
+size_t walk_args_bytes() { return sizeof(WalkArgs); }
 
 int state_slots() { return kStN; }
 int slot_r() { return kStR; }

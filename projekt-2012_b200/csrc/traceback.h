@@ -37,6 +37,12 @@ struct WalkInputs {
     int64_t *dstate;              // device copy of the walker state
 };
 int walk_region(cudaStream_t st, const WalkInputs &in, int64_t *host_state, std::string &err);
+// Walks n independent pairs (each region is its pair's whole matrix) with one
+// launch; d_args holds n * walk_args_bytes() bytes, d_states n * state_slots()
+// int64 (initial states are copied from host_states, final ones back to it).
+int walk_batch(cudaStream_t st, int sms, const WalkInputs *in, int64_t n, void *d_args, int64_t *d_states,
+               int64_t *host_states, std::string &err);
+size_t walk_args_bytes();
 int state_slots();
 int slot_r();
 int slot_c();

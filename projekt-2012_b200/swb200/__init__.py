@@ -52,6 +52,28 @@ class Result(C.Structure):
                 ("special_bytes", C.c_int64), ("kernel_launches", C.c_int32)]
 
 
+class PairRef(C.Structure):
+    _fields_ = [("a_off", C.c_int64), ("a_len", C.c_int64), ("b_off", C.c_int64), ("b_len", C.c_int64)]
+
+
+class BatchItem(C.Structure):
+    _fields_ = [("score", C.c_int32), ("swapped", C.c_int32),
+                ("end_row", C.c_int64), ("end_col", C.c_int64),
+                ("start_row", C.c_int64), ("start_col", C.c_int64),
+                ("ops_off", C.c_int64), ("n_ops", C.c_int64),
+                ("xp_off", C.c_int64), ("n_xpoints", C.c_int64),
+                ("traced", C.c_int32), ("xpoint_interval", C.c_int32)]
+
+
+class BatchResult(C.Structure):
+    _fields_ = [("npairs", C.c_int64), ("items", C.POINTER(BatchItem)),
+                ("ops", C.c_void_p), ("ops_bytes", C.c_int64),
+                ("xpoints", C.POINTER(XPoint)), ("n_xpoints", C.c_int64),
+                ("n_traced", C.c_int64), ("cells", C.c_int64),
+                ("stage1_ms", C.c_double), ("stage2_ms", C.c_double), ("total_ms", C.c_double),
+                ("kernel_launches", C.c_int32)]
+
+
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64),
                 ("special_interval", C.c_int32), ("verbose", C.c_int32),
@@ -98,6 +120,12 @@ def lib():
                                            C.POINTER(C.c_int64)]
         L.swb_special_row_copy.restype = C.c_int
         L.swb_version.restype = C.c_char_p
+        L.swb_batch_align.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                      C.POINTER(Scoring), C.c_uint32, C.c_double, C.POINTER(BatchResult)]
+        L.swb_batch_align.restype = C.c_int
+        L.swb_batch_align_device.argtypes = L.swb_batch_align.argtypes
+        L.swb_batch_align_device.restype = C.c_int
+        L.swb_batch_result_free.argtypes = [C.POINTER(BatchResult)]
         L.swb_probe_cell_peak.argtypes = [C.c_int32] + [C.POINTER(C.c_double)] * 5
         L.swb_probe_cell_peak.restype = C.c_int
         L.swb_probe_latency.argtypes = [C.c_int32, C.POINTER(C.c_double), C.c_int32]
@@ -130,6 +158,67 @@ class Alignment:
     special_bytes: int = 0
     kernel_launches: int = 0
     n_ops: int = 0
+
+
+@dataclass
+class Batch:
+    """Result of a batched call: per-pair arrays in the order of the pairs
+    argument, and the alignments / crosspoints of the traced pairs."""
+    score: "object"            # numpy int32 [n]
+    end_row: "object"          # numpy int64 [n]
+    end_col: "object"
+    start_row: "object"
+    start_col: "object"
+    swapped: "object"
+    traced: "object"
+    ops: List[str]             # "" for pairs that were not traced
+    xpoints: List[list]        # [] for pairs that were not traced
+    xpoint_interval: "object"
+    n_traced: int
+    cells: int
+    stage1_ms: float
+    stage2_ms: float
+    total_ms: float
+    kernel_launches: int
+
+
+def _convert_batch(r: BatchResult) -> Batch:
+    import numpy as np
+    n = r.npairs
+    items = np.ctypeslib.as_array(C.cast(r.items, C.POINTER(C.c_int64)),
+                                 shape=(n * C.sizeof(BatchItem) // 8,)).copy() if n else np.zeros(0, np.int64)
+    raw = items.view(np.uint8).reshape(n, C.sizeof(BatchItem)) if n else np.zeros((0, C.sizeof(BatchItem)), np.uint8)
+    def col(name, dt):
+        off = getattr(BatchItem, name).offset
+        size = np.dtype(dt).itemsize
+        return raw[:, off:off + size].copy().view(dt).reshape(n)
+    score, swapped = col("score", np.int32), col("swapped", np.int32)
+    traced, xpi = col("traced", np.int32), col("xpoint_interval", np.int32)
+    ops_off, n_ops = col("ops_off", np.int64), col("n_ops", np.int64)
+    xp_off, n_xp = col("xp_off", np.int64), col("n_xpoints", np.int64)
+    allops = C.string_at(r.ops, r.ops_bytes).decode() if r.ops and r.ops_bytes > 0 else ""
+    ops, xps = [], []
+    for i in range(n):
+        if traced[i]:
+            ops.append(allops[ops_off[i]:ops_off[i] + n_ops[i]])
+            xps.append([(r.xpoints[k].row, r.xpoints[k].col, r.xpoints[k].score, r.xpoints[k].gap)
+                        for k in range(xp_off[i], xp_off[i] + n_xp[i])])
+        else:
+            ops.append("")
+            xps.append([])
+    return Batch(score, col("end_row", np.int64), col("end_col", np.int64), col("start_row", np.int64),
+                 col("start_col", np.int64), swapped.astype(bool), traced.astype(bool), ops, xps, xpi,
+                 r.n_traced, r.cells, r.stage1_ms, r.stage2_ms, r.total_ms, r.kernel_launches)
+
+
+def pair_refs(refs) -> "C.Array":
+    """(n, 4) int64 array of (a_off, a_len, b_off, b_len) -> ctypes array of PairRef."""
+    import numpy as np
+    a = np.ascontiguousarray(refs, dtype=np.int64).reshape(-1, 4)
+    arr = (PairRef * len(a))()
+    if len(a):
+        C.memmove(arr, a.ctypes.data, a.nbytes)
+    return arr
 
 
 def _convert(r: Result) -> Alignment:
@@ -215,6 +304,29 @@ class Context:
             return _convert(r)
         finally:
             lib().swb_result_free(C.byref(r))
+
+    def batch_align(self, seq, refs, sc: Scoring, flags: int = 0, trace_frac: float = 0.0,
+                    seq_ptr: Optional[int] = None, device: bool = False) -> Batch:
+        """Aligns the pairs refs[i] = (a_off, a_len, b_off, b_len) of the buffer seq
+        (bytes / numpy uint8), or of the buffer at address seq_ptr (host memory, or
+        device memory when device=True, len(seq) bytes when seq is an int)."""
+        import numpy as np
+        pr = pair_refs(refs)
+        if seq_ptr is None:
+            buf = np.frombuffer(seq, dtype=np.uint8) if isinstance(seq, (bytes, bytearray)) else \
+                np.ascontiguousarray(seq, dtype=np.uint8)
+            ptr, nbytes = buf.ctypes.data, buf.nbytes
+        else:
+            ptr, nbytes = seq_ptr, int(seq)
+        r = BatchResult()
+        fn = lib().swb_batch_align_device if device else lib().swb_batch_align
+        rc = fn(self._h, C.c_void_p(ptr), nbytes, pr, len(pr), C.byref(sc), flags, trace_frac, C.byref(r))
+        if rc != SWB_OK:
+            self._err(rc)
+        try:
+            return _convert_batch(r)
+        finally:
+            lib().swb_batch_result_free(C.byref(r))
 
     def trace(self):
         """Stage-1 strip trace of the last call: numpy array [strips, 3] of

@@ -78,3 +78,28 @@ def chromosome_pair(ancestor: int = 8_000_000, flank: int = 1_000_000, seed_extr
     a = np.concatenate([random_dna(rng, flank), mutate(rng, anc, 0.03, 0.005, 4.0), random_dna(rng, flank)])
     b = np.concatenate([random_dna(rng, flank), mutate(rng, anc, 0.03, 0.005, 4.0), random_dna(rng, flank)])
     return a.tobytes(), b.tobytes(), (1, -3, -5, -2)
+
+
+def batched(npairs: int = 100_000, seed_extra: int = 0, sigma: float = 0.75):
+    """Batched workload: query lengths clip(round(lognormal(ln 1000, sigma)), 100,
+    10,000); each target is 1.5x its query long, built from mutate(query, 8% sub,
+    1% indel, mean 3) placed at a uniform random offset inside random padding.
+    Returns (buffer, refs, scoring): one uint8 buffer holding every query and
+    target, refs[i] = (query_off, query_len, target_off, target_len)."""
+    rng = rng_for(3, seed_extra)
+    q = np.clip(np.round(rng.lognormal(np.log(1000.0), sigma, size=npairs)), 100, 10_000).astype(np.int64)
+    parts, refs, off = [], np.zeros((npairs, 4), dtype=np.int64), 0
+    for i, L in enumerate(q.tolist()):
+        query = random_dna(rng, L)
+        core = mutate(rng, query, 0.08, 0.01, 3.0)
+        tlen = int(round(1.5 * L))
+        if len(core) > tlen:
+            core = core[:tlen]
+        pad = tlen - len(core)
+        left = int(rng.integers(0, pad + 1))
+        target = np.concatenate([random_dna(rng, left), core, random_dna(rng, pad - left)])
+        refs[i] = (off, L, off + L, tlen)
+        parts.append(query)
+        parts.append(target)
+        off += L + tlen
+    return np.concatenate(parts), refs, (2, -3, -5, -2)
