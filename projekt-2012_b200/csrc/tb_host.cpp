@@ -57,8 +57,7 @@ int traceback(cudaStream_t st, int sms, const uint8_t *d_rows, int64_t m, const 
         w.rtop = nullptr;
         w.rleft = nullptr;
         w.rcorner = 0;
-        if ((rc = walk_region(st, w, S.data(), err)) != SWB_OK) return rc;
-        *launches += 1;
+        if ((rc = walk_region(st, sms, w, S.data(), scr, err, launches)) != SWB_OK) return rc;
     } else {
         // level 1: walk level-1 cell after level-1 cell
         for (int guard = 0; guard < (1 << 24) && !S[slot_done()]; ++guard) {
@@ -138,8 +137,7 @@ int traceback(cudaStream_t st, int sms, const uint8_t *d_rows, int64_t m, const 
             w.rtop = top;
             w.rleft = left;
             w.rcorner = corner;
-            if ((rc = walk_region(st, w, S.data(), err)) != SWB_OK) return rc;
-            *launches += 1;
+            if ((rc = walk_region(st, sms, w, S.data(), scr, err, launches)) != SWB_OK) return rc;
         }
         if (!S[slot_done()]) {
             err = "traceback did not finish";

@@ -21,6 +21,7 @@
 // each level-1 cell the path enters is recomputed by the stage-1 kernel on that
 // sub-rectangle, which writes the 512 x 256 stores for it (level 2).
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -103,14 +104,106 @@ __device__ void stage_block(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C
     for (int64_t i = threadIdx.x; i < h; i += blockDim.x) s->rb[i] = a.rows[R0 + i];
 }
 
-// Recomputes block rows [R0, R1] x cols [C0, C1] into dir (row-major, kBC wide).
-// Expects stage_block() to have filled `s` (and a barrier after it).
-__device__ void recompute(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0, int64_t C1, uint8_t *dir,
-                          int2 (*xchg)[kThreads / 32], const Stage *s) {
+// Direction byte of block cell (row offset i, column offset j): column-major, so
+// the kRT rows a lane computes for one column are one aligned 32-bit word.
+__device__ __forceinline__ int dix(int64_t i, int64_t j) { return (int)(j * kBR + i); }
+
+// Direction bytes of the block being walked, in shared memory (column-major).
+struct SmemDir {
+    uint8_t *d;
+    __device__ __forceinline__ uint8_t at(int64_t i, int64_t j) const { return d[dix(i, j)]; }
+    __device__ __forceinline__ void put(int t, int64_t j, int64_t /*k*/, uint32_t word) const {
+        *reinterpret_cast<uint32_t *>(d + dix(4 * t, j)) = word;
+    }
+};
+
+// Direction bytes of one precomputed block in global memory, in the recompute's
+// step order so that every warp store is one coalesced 128-byte line: word
+// (warp, k, lane) holds rows 4t .. 4t + 3 (t = 32 warp + lane) of column k - lane.
+constexpr int kSteps = kBC + 31;
+constexpr int64_t kBlockWords = (int64_t)(kThreads / 32) * kSteps * 32;
+struct GlobalDir {
+    uint32_t *d;
+    __device__ __forceinline__ uint8_t at(int64_t i, int64_t j) const {
+        const int t = (int)(i >> 2), lane = t & 31, warp = t >> 5;
+        const int64_t k = j + lane;
+        return reinterpret_cast<const uint8_t *>(d + ((int64_t)warp * kSteps + k) * 32 + lane)[i & 3];
+    }
+    __device__ __forceinline__ void put(int t, int64_t /*j*/, int64_t k, uint32_t word) const {
+        d[((int64_t)(t >> 5) * kSteps + k) * 32 + (t & 31)] = word;
+    }
+};
+
+// Hand-off between the warps of a recompute: warp w publishes (H, F) of its last
+// row (block row 128 (w + 1) - 1) column by column in bnd[w][j] as two 64-bit
+// words {H, gen} and {F, gen}, gen being the recompute's generation; warp w + 1
+// reads them as the row above and re-reads until both tags show the current
+// generation.  A 64-bit shared access is single-copy atomic, so the tag proves its
+// value is current without any fence.
+struct Xchg {
+    unsigned long long bnd[kThreads / 32 - 1][kBC][2];
+    int32_t err;
+    uint32_t gen;  // generations used so far by this CTA (tags start at 1; entries start at 0)
+};
+
+// Zeroes the hand-off tags and the generation count (once per CTA).
+__device__ void xchg_init(Xchg *x) {
+    unsigned long long *p = &x->bnd[0][0][0];
+    for (int i = threadIdx.x; i < (kThreads / 32 - 1) * kBC * 2; i += blockDim.x) p[i] = 0ULL;
+    if (threadIdx.x == 0) {
+        x->err = 0;
+        x->gen = 0;
+    }
+}
+
+// Upper bound of a warp's wait for the warp above (SM cycles, about 1 s); the
+// writer is a warp of the same CTA, so this only guards against a defect.
+constexpr long long kXchgWaitCycles = 2LL * 1000 * 1000 * 1000;
+
+__device__ __forceinline__ unsigned long long pack(int32_t v, uint32_t gen) {
+    return ((unsigned long long)gen << 32) | (uint32_t)v;
+}
+__device__ __forceinline__ unsigned long long ld_shared_volatile(const unsigned long long *p) {
+    return *reinterpret_cast<const volatile unsigned long long *>(p);
+}
+
+// Waits until entry j of boundary b carries generation gen; returns (H, F).  After
+// one wait ran out (x->err set) it no longer waits: the warp finishes its loop on
+// whatever values it reads and the caller discards the block.
+__device__ __forceinline__ int2 take(Xchg *x, int b, int64_t j, uint32_t gen, bool &fail) {
+    if (fail) return make_int2(0, 0);
+    unsigned long long h = ld_shared_volatile(&x->bnd[b][j][0]);
+    unsigned long long f = ld_shared_volatile(&x->bnd[b][j][1]);
+    if ((uint32_t)(h >> 32) != gen || (uint32_t)(f >> 32) != gen) {
+        const long long t0 = clock64();
+        for (;;) {
+            h = ld_shared_volatile(&x->bnd[b][j][0]);
+            f = ld_shared_volatile(&x->bnd[b][j][1]);
+            if ((uint32_t)(h >> 32) == gen && (uint32_t)(f >> 32) == gen) break;
+            if (clock64() - t0 > kXchgWaitCycles) {
+                fail = true;
+                x->err = 1;
+                break;
+            }
+        }
+    }
+    return make_int2((int32_t)(uint32_t)h, (int32_t)(uint32_t)f);
+}
+
+// Recomputes block rows [R0, R1] x cols [C0, C1] into dir.  Expects
+// stage_block() to have filled `s`, x->err zeroed, and a barrier after both;
+// `gen` must differ from every earlier recompute of this CTA.  Thread t owns
+// rows R0 + 4t .. R0 + 4t + 3: each warp is a 128-row wavefront (lane l computes
+// column k - l at step k, rows passed down by shuffles) and the four warps form
+// a pipeline through x, so no CTA barrier is needed inside the column loop.
+template <class D>
+__device__ void recompute(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0, int64_t C1, const D &dir,
+                          Xchg *x, const Stage *s, uint32_t gen) {
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
     const int64_t w = C1 - C0 + 1;
     const int64_t r0 = R0 + (int64_t)t * kRT;  // my first row
+    if (R0 + (int64_t)warp * 32 * kRT > R1) return;  // this warp (and every warp below it) has no rows
     int32_t Hl[kRT], El[kRT];
     uint8_t ra[kRT];
 #pragma unroll
@@ -131,14 +224,19 @@ __device__ void recompute(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0,
     int32_t hdiag0;
     if (t == 0) hdiag0 = s->top[0].x;
     else hdiag0 = (r0 - 1 <= R1) ? left_he(a, C0, r0 - 1).x : 0;
+    bool fail = false;
+    // warps below the first start with a few columns of slack behind the warp above
+    if (warp > 0 && lane == 0) take(x, warp - 1, w - 1 < 15 ? w - 1 : 15, gen, fail);
+    __syncwarp();
     int32_t upH = 0, upF = 0;  // (H, F) from the row above at my current column
     int32_t prevUpH = hdiag0;  // H of the row above at the previous column
-    const int64_t steps = w + kThreads - 1;
+    const bool publish = (lane == 31) && warp < kThreads / 32 - 1 && (r0 + kRT - 1 <= R1);
+    const int64_t steps = w + 31;
     for (int64_t k = 0; k < steps; ++k) {
-        const int64_t j = k - t;  // my column offset
+        const int64_t j = k - lane;  // my column offset
         const bool act = (j >= 0 && j < w && r0 <= R1);
-        if (t == 0 && j >= 0 && j < w) {
-            const int2 tv = s->top[j + 1];
+        if (lane == 0 && j < w) {
+            const int2 tv = (warp == 0) ? s->top[j + 1] : take(x, warp - 1, j, gen, fail);
             upH = tv.x;
             upF = tv.y;
         }
@@ -147,53 +245,50 @@ __device__ void recompute(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0,
             const uint8_t cb = s->cb[j];
             int32_t hd = prevUpH;
             int32_t hu = upH, fu = upF;
+            uint32_t word = 0;
 #pragma unroll
             for (int i = 0; i < kRT; ++i) {
-                if (r0 + i > R1) break;
-                const int32_t eext = El[i] + a.ext, eopen = Hl[i] + a.open;
-                const int32_t fext = fu + a.ext, fopen = hu + a.open;
-                const int32_t e = max(eext, eopen), f = max(fext, fopen);
-                const int32_t dg = hd + (ra[i] == cb ? a.match : a.mismatch);
-                const int32_t hv = max(max(0, e), max(f, dg));
-                uint8_t v = hv == 0 ? SRC_ZERO : (hv == dg ? SRC_DIAG : (hv == e ? SRC_E : SRC_F));
-                if (eext == e) v |= BIT_EEXT;
-                if (fext == f) v |= BIT_FEXT;
-                if (hd == 0) v |= BIT_DZERO;
-                dir[(r0 + i - R0) * kBC + j] = v;
-                hd = Hl[i];
-                Hl[i] = hv;
-                El[i] = e;
-                hu = hv;
-                fu = f;
+                if (r0 + i <= R1) {
+                    const int32_t eext = El[i] + a.ext, eopen = Hl[i] + a.open;
+                    const int32_t fext = fu + a.ext, fopen = hu + a.open;
+                    const int32_t e = max(eext, eopen), f = max(fext, fopen);
+                    const int32_t dg = hd + (ra[i] == cb ? a.match : a.mismatch);
+                    const int32_t hv = max(max(0, e), max(f, dg));
+                    uint32_t v = hv == 0 ? SRC_ZERO : (hv == dg ? SRC_DIAG : (hv == e ? SRC_E : SRC_F));
+                    if (eext == e) v |= BIT_EEXT;
+                    if (fext == f) v |= BIT_FEXT;
+                    if (hd == 0) v |= BIT_DZERO;
+                    word |= v << (8 * i);
+                    hd = Hl[i];
+                    Hl[i] = hv;
+                    El[i] = e;
+                    hu = hv;
+                    fu = f;
+                }
             }
+            dir.put(t, j, k, word);
             oH = hu;
             oF = fu;
+            if (publish) {
+                x->bnd[warp][j][0] = pack(oH, gen);
+                x->bnd[warp][j][1] = pack(oF, gen);
+            }
         }
         prevUpH = upH;
-        // hand (H, F) of my last row to the thread below for the next step; the
-        // cross-warp slot alternates between two buffers so one barrier per step
-        // orders both the write of step k and the reuse of the slot at step k + 2
+        // hand (H, F) of my last row to the lane below for the next step
         const int32_t sH = __shfl_up_sync(0xffffffffu, oH, 1);
         const int32_t sF = __shfl_up_sync(0xffffffffu, oF, 1);
-        int2 *xb = xchg[k & 1];
-        if (lane == 31) xb[warp] = make_int2(oH, oF);
-        __syncthreads();
-        if (t > 0) {
-            if (lane == 0) {
-                const int2 v = xb[warp - 1];
-                upH = v.x;
-                upF = v.y;
-            } else {
-                upH = sH;
-                upF = sF;
-            }
+        if (lane > 0) {
+            upH = sH;
+            upF = sF;
             if (j + 1 == 0) prevUpH = hdiag0;  // my first column: diagonal from the left boundary
         }
     }
 }
 
 // Warp 0 walks the path through the block [R0, R1] x [C0, C1].
-__device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const uint8_t *dir, const Stage *sg, int64_t *S) {
+template <class D>
+__device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const D &dir, const Stage *sg, int64_t *S) {
     const int lane = threadIdx.x & 31;
     int64_t r = S[kStR], c = S[kStC];
     int32_t state = (int32_t)S[kStState];
@@ -205,7 +300,7 @@ __device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const uint8_t *d
             // run of diagonal moves that are not the start
             const int64_t rr = r - lane, cc = c - lane;
             const bool in = rr >= R0 && cc >= C0;
-            const uint8_t v = in ? dir[(rr - R0) * kBC + (cc - C0)] : 0;
+            const uint8_t v = in ? dir.at(rr - R0, cc - C0) : 0;
             const bool ok = in && (v & 3) == SRC_DIAG && !(v & BIT_DZERO);
             const uint32_t bal = __ballot_sync(0xffffffffu, ok);
             const int nrun = (bal == 0xffffffffu) ? 32 : __ffs(~bal) - 1;
@@ -239,7 +334,7 @@ __device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const uint8_t *d
             r -= nrun;
             c -= nrun;
             if (nrun < 32 && r >= R0 && c >= C0) {
-                const uint8_t w = dir[(r - R0) * kBC + (c - C0)];
+                const uint8_t w = dir.at(r - R0, c - C0);
                 const int src = w & 3;
                 if (src == SRC_DIAG) {  // the start cell
                     if (lane == 0 && nops < a.ops_cap) a.ops[nops] = 'M';
@@ -260,7 +355,7 @@ __device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const uint8_t *d
             // horizontal run: 'I' for every cell until the gap opens
             const int64_t cc = c - lane;
             const bool in = cc >= C0;
-            const uint8_t v = in ? dir[(r - R0) * kBC + (cc - C0)] : 0;
+            const uint8_t v = in ? dir.at(r - R0, cc - C0) : 0;
             const bool ext = in && (v & BIT_EEXT);
             const uint32_t bal = __ballot_sync(0xffffffffu, ext);
             const uint32_t inb = __ballot_sync(0xffffffffu, in);
@@ -283,7 +378,7 @@ __device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const uint8_t *d
             // vertical run: 'D' for every cell until the gap opens
             const int64_t rr = r - lane;
             const bool in = rr >= R0;
-            const uint8_t v = in ? dir[(rr - R0) * kBC + (c - C0)] : 0;
+            const uint8_t v = in ? dir.at(rr - R0, c - C0) : 0;
             const bool ext = in && (v & BIT_FEXT);
             const uint32_t bal = __ballot_sync(0xffffffffu, ext);
             const uint32_t inb = __ballot_sync(0xffffffffu, in);
@@ -336,46 +431,109 @@ __device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const uint8_t *d
 
 // Block after block until the start is reached or the path leaves the region
 // [rr0, .) x [cc0, .); the state is read from and written back to a.st.
-__device__ void walk_body(const WalkArgs &a, uint8_t *dir, int2 (*xchg)[kThreads / 32], Stage *sg, int64_t *S) {
+__device__ void walk_body(const WalkArgs &a, uint8_t *dir, Xchg *xc, Stage *sg, int64_t *S) {
     if (threadIdx.x < kStN) S[threadIdx.x] = a.st[threadIdx.x];
     __syncthreads();
-    for (int guard = 0; guard < (1 << 30); ++guard) {
+    int guard = 0;
+    for (; guard < (1 << 30); ++guard) {
         const int64_t r = S[kStR], c = S[kStC];
         if (S[kStDone] || S[kStErr] || r < a.rr0 || c < a.cc0) break;
         const int64_t R0 = a.rr0 + ((r - a.rr0) / kBR) * kBR;
         const int64_t C0 = a.cc0 + ((c - a.cc0) / kBC) * kBC;
         stage_block(a, R0, r, C0, c, sg);
         __syncthreads();
-        recompute(a, R0, r, C0, c, dir, xchg, sg);
+        recompute(a, R0, r, C0, c, SmemDir{dir}, xc, sg, xc->gen + (uint32_t)guard + 1u);
         __syncthreads();
-        if (threadIdx.x < 32) walk(a, R0, C0, dir, sg, S);
+        if (xc->err) {
+            if (threadIdx.x == 0) S[kStErr] = 1;
+            __syncthreads();
+            break;
+        }
+        if (threadIdx.x < 32) walk(a, R0, C0, SmemDir{dir}, sg, S);
         __syncthreads();
     }
     if (threadIdx.x < kStN) a.st[threadIdx.x] = S[threadIdx.x];
+    __syncthreads();
+    if (threadIdx.x == 0) xc->gen += (uint32_t)guard + 1u;  // generations used by this region
 }
 
-// One CTA walks one region.
-__global__ void __launch_bounds__(kThreads) walk_kernel(WalkArgs a) {
-    extern __shared__ uint8_t dir[];
-    __shared__ int2 xchg[2][kThreads / 32];
+// Precomputes the direction bytes of whole blocks (R0, C0) = blk[2b], blk[2b + 1]
+// of a region into gdir + b * kBlockWords (one CTA per block at a time).  A block
+// depends only on the stored boundaries, not on the path, so any set of blocks
+// can run at once.
+__global__ void __launch_bounds__(kThreads) precompute_kernel(WalkArgs a, const int64_t *blk, int64_t nblk,
+                                                              uint32_t *gdir, int32_t *err) {
+    __shared__ Xchg xc;
+    __shared__ Stage sg;
+    xchg_init(&xc);
+    uint32_t gen = 0;
+    for (int64_t b = blockIdx.x; b < nblk; b += gridDim.x) {
+        const int64_t R0 = blk[2 * b], C0 = blk[2 * b + 1];
+        const int64_t R1 = min(R0 + kBR - 1, a.rr1 - 1), C1 = min(C0 + kBC - 1, a.cc1 - 1);
+        __syncthreads();
+        stage_block(a, R0, R1, C0, C1, &sg);
+        __syncthreads();
+        recompute(a, R0, R1, C0, C1, GlobalDir{gdir + b * kBlockWords}, &xc, &sg, ++gen);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && xc.err) atomicExch(err, 1);
+}
+
+// Sequence bytes of a block for the walk's diagonal scores.
+__device__ void stage_bytes(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0, int64_t C1, Stage *s) {
+    for (int64_t j = threadIdx.x; j <= C1 - C0; j += blockDim.x) s->cb[j] = a.cols[C0 + j];
+    for (int64_t i = threadIdx.x; i <= R1 - R0; i += blockDim.x) s->rb[i] = a.rows[R0 + i];
+}
+
+// One warp walks the path through precomputed blocks: block (bi, bj) of the
+// region (relative to rr0, cc0) is slot map[(bi - bi0) * mw + (bj - bj0)] of
+// gdir, or absent (-1).  Stops where the path enters an absent block, at the
+// start cell or on an error; the state is read from and written back to a.st.
+__global__ void __launch_bounds__(32) corridor_walk_kernel(WalkArgs a, const uint32_t *gdir, const int32_t *map,
+                                                           int64_t bi0, int64_t bj0, int64_t mh, int64_t mw,
+                                                           const int32_t *err) {
     __shared__ Stage sg;
     __shared__ int64_t S[kStN];
-    walk_body(a, dir, xchg, &sg, S);
+    if (threadIdx.x < kStN) S[threadIdx.x] = a.st[threadIdx.x];
+    __syncwarp();
+    if (*err) {
+        if (threadIdx.x == 0) S[kStErr] = 1;
+        __syncwarp();
+    }
+    for (;;) {
+        const int64_t r = S[kStR], c = S[kStC];
+        if (S[kStDone] || S[kStErr] || r < a.rr0 || c < a.cc0) break;
+        const int64_t bi = (r - a.rr0) / kBR, bj = (c - a.cc0) / kBC;
+        if (bi < bi0 || bi >= bi0 + mh || bj < bj0 || bj >= bj0 + mw) break;
+        const int32_t slot = map[(bi - bi0) * mw + (bj - bj0)];
+        if (slot < 0) break;
+        const int64_t R0 = a.rr0 + bi * kBR, C0 = a.cc0 + bj * kBC;
+        stage_bytes(a, R0, r, C0, c, &sg);
+        __syncwarp();
+        walk(a, R0, C0, GlobalDir{const_cast<uint32_t *>(gdir) + (int64_t)slot * kBlockWords}, &sg, S);
+        __syncwarp();
+    }
+    __syncwarp();
+    if (threadIdx.x < kStN) a.st[threadIdx.x] = S[threadIdx.x];
 }
 
 // Batched pairs: CTA b walks pairs b, b + gridDim.x, ... (each pair's whole
 // matrix is its region).
 __global__ void __launch_bounds__(kThreads) walk_batch_kernel(const WalkArgs *args, int64_t n) {
     extern __shared__ uint8_t dir[];
-    __shared__ int2 xchg[2][kThreads / 32];
+    __shared__ Xchg xc;
     __shared__ Stage sg;
     __shared__ int64_t S[kStN];
     __shared__ WalkArgs sa;
+    xchg_init(&xc);
     for (int64_t p = blockIdx.x; p < n; p += gridDim.x) {
         __syncthreads();
-        if (threadIdx.x == 0) sa = args[p];
+        if (threadIdx.x == 0) {
+            sa = args[p];
+            xc.err = 0;
+        }
         __syncthreads();
-        walk_body(sa, dir, xchg, &sg, S);
+        walk_body(sa, dir, &xc, &sg, S);
     }
 }
 
@@ -437,28 +595,108 @@ static WalkArgs to_args(const WalkInputs &in) {
     return a;
 }
 
-int walk_region(cudaStream_t st, const WalkInputs &in, int64_t *host_state, std::string &err) {
+// Blocks the path is expected to cross next: the staircase of blocks along the
+// diagonal from the current cell toward the region's origin (a local alignment
+// of related sequences runs close to a diagonal), with the block above and the
+// block to the left of each as margin, in walk order, at most `cap` of them.
+static void predict_corridor(const WalkInputs &in, int64_t r, int64_t c, int64_t cap, std::vector<int64_t> &blk,
+                             int64_t &bi0, int64_t &bj0, int64_t &mh, int64_t &mw, std::vector<int32_t> &map) {
+    std::vector<std::pair<int64_t, int64_t>> list;
+    auto add = [&](int64_t bi, int64_t bj) {
+        if (bi < 0 || bj < 0 || (int64_t)list.size() >= cap) return;
+        for (size_t q = list.size() >= 8 ? list.size() - 8 : 0; q < list.size(); ++q)
+            if (list[q].first == bi && list[q].second == bj) return;
+        list.emplace_back(bi, bj);
+    };
+    int64_t bi = (r - in.rr0) / kBR, bj = (c - in.cc0) / kBC;
+    add(bi, bj);
+    add(bi - 1, bj);
+    add(bi, bj - 1);
+    while ((int64_t)list.size() < cap) {
+        const int64_t R0 = in.rr0 + bi * kBR, C0 = in.cc0 + bj * kBC;
+        const int64_t d = std::min(r - R0 + 1, c - C0 + 1);
+        r -= d;
+        c -= d;
+        if (r < in.rr0 || c < in.cc0) break;
+        bi = (r - in.rr0) / kBR;
+        bj = (c - in.cc0) / kBC;
+        add(bi, bj);
+        add(bi - 1, bj);
+        add(bi, bj - 1);
+    }
+    int64_t bmin = INT64_MAX, bmax = -1, cmin = INT64_MAX, cmax = -1;
+    for (auto &p : list) {
+        bmin = std::min(bmin, p.first);
+        bmax = std::max(bmax, p.first);
+        cmin = std::min(cmin, p.second);
+        cmax = std::max(cmax, p.second);
+    }
+    bi0 = bmin;
+    bj0 = cmin;
+    mh = bmax - bmin + 1;
+    mw = cmax - cmin + 1;
+    map.assign((size_t)(mh * mw), -1);
+    blk.resize(2 * list.size());
+    for (size_t q = 0; q < list.size(); ++q) {
+        int32_t &slot = map[(size_t)((list[q].first - bi0) * mw + (list[q].second - bj0))];
+        if (slot < 0) slot = (int32_t)q;
+        blk[2 * q] = in.rr0 + list[q].first * kBR;
+        blk[2 * q + 1] = in.cc0 + list[q].second * kBC;
+    }
+}
+
+int walk_region(cudaStream_t st, int sms, const WalkInputs &in, int64_t *host_state, const Scratch &scr,
+                std::string &err, int32_t *launches) {
     const WalkArgs a = to_args(in);
     cudaError_t e;
-    const size_t smem = (size_t)kBR * kBC;
-    // the attribute is per device: set it on every call (cheap)
-    if ((e = cudaFuncSetAttribute(walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
-        cudaSuccess) {
-        err = std::string("walker attribute: ") + cudaGetErrorString(e);
-        return SWB_ECUDA;
+    const int64_t cap = 4LL * std::max(1, sms);  // blocks per round: one wave at four CTAs per SM
+    uint32_t *gdir = (uint32_t *)scr.ensure(scr.owner, kScrGdir, sizeof(uint32_t) * (size_t)(cap * kBlockWords));
+    int64_t *d_blk = (int64_t *)scr.ensure(scr.owner, kScrBlk, sizeof(int64_t) * 2 * (size_t)cap);
+    int32_t *d_err = (int32_t *)scr.ensure(scr.owner, kScrWalkErr, sizeof(int32_t));
+    if (!gdir || !d_blk || !d_err) {
+        err = "walker buffers: out of device memory";
+        return SWB_ENOMEM;
     }
-    if ((e = cudaMemcpyAsync(in.dstate, host_state, sizeof(int64_t) * kStN, cudaMemcpyHostToDevice, st)) !=
-        cudaSuccess) {
+    if ((e = cudaMemsetAsync(d_err, 0, sizeof(int32_t), st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(in.dstate, host_state, sizeof(int64_t) * kStN, cudaMemcpyHostToDevice, st)) !=
+            cudaSuccess) {
         err = std::string("walker state: ") + cudaGetErrorString(e);
         return SWB_ECUDA;
     }
-    walk_kernel<<<1, kThreads, smem, st>>>(a);
-    if ((e = cudaGetLastError()) != cudaSuccess ||
-        (e = cudaMemcpyAsync(host_state, in.dstate, sizeof(int64_t) * kStN, cudaMemcpyDeviceToHost, st)) !=
-            cudaSuccess ||
-        (e = cudaStreamSynchronize(st)) != cudaSuccess) {
-        err = std::string("walker: ") + cudaGetErrorString(e);
-        return SWB_ECUDA;
+    std::vector<int64_t> blk;
+    std::vector<int32_t> map;
+    for (int round = 0; round < (1 << 26); ++round) {
+        const int64_t r = host_state[kStR], c = host_state[kStC];
+        if (host_state[kStDone] || host_state[kStErr] || r < in.rr0 || c < in.cc0) break;
+        int64_t bi0, bj0, mh, mw;
+        predict_corridor(in, r, c, cap, blk, bi0, bj0, mh, mw, map);
+        const int64_t nblk = (int64_t)blk.size() / 2;
+        int32_t *d_map = (int32_t *)scr.ensure(scr.owner, kScrMap, sizeof(int32_t) * map.size());
+        if (!d_map) {
+            err = "walker buffers: out of device memory";
+            return SWB_ENOMEM;
+        }
+        if ((e = cudaMemcpyAsync(d_blk, blk.data(), sizeof(int64_t) * blk.size(), cudaMemcpyHostToDevice, st)) !=
+                cudaSuccess ||
+            (e = cudaMemcpyAsync(d_map, map.data(), sizeof(int32_t) * map.size(), cudaMemcpyHostToDevice, st)) !=
+                cudaSuccess) {
+            err = std::string("walker corridor: ") + cudaGetErrorString(e);
+            return SWB_ECUDA;
+        }
+        precompute_kernel<<<(unsigned)nblk, kThreads, 0, st>>>(a, d_blk, nblk, gdir, d_err);
+        corridor_walk_kernel<<<1, 32, 0, st>>>(a, gdir, d_map, bi0, bj0, mh, mw, d_err);
+        *launches += 2;
+        if ((e = cudaGetLastError()) != cudaSuccess ||
+            (e = cudaMemcpyAsync(host_state, in.dstate, sizeof(int64_t) * kStN, cudaMemcpyDeviceToHost, st)) !=
+                cudaSuccess ||
+            (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+            err = std::string("walker: ") + cudaGetErrorString(e);
+            return SWB_ECUDA;
+        }
+        if (host_state[kStR] == r && host_state[kStC] == c && !host_state[kStDone] && !host_state[kStErr]) {
+            err = "walker: no progress through the current block";
+            return SWB_ECUDA;
+        }
     }
     if (host_state[kStErr]) {
         err = "walker: inconsistent direction data";

@@ -36,7 +36,7 @@ struct WalkInputs {
     int64_t xp_cap;
     int64_t *dstate;              // device copy of the walker state
 };
-int walk_region(cudaStream_t st, const WalkInputs &in, int64_t *host_state, std::string &err);
+
 // Walks n independent pairs (each region is its pair's whole matrix) with one
 // launch; d_args holds n * walk_args_bytes() bytes, d_states n * state_slots()
 // int64 (initial states are copied from host_states, final ones back to it).
@@ -60,7 +60,16 @@ struct Scratch {
     void *(*ensure)(void *owner, int which, size_t bytes);  // returns device memory or nullptr
     void *owner;
 };
-enum ScratchSlot { kScrOps = 0, kScrXps, kScrState, kScrSrows2, kScrScols2, kScrHbuf, kScrWbest, kScrBest, kScrErr };
+enum ScratchSlot {
+    kScrOps = 0, kScrXps, kScrState, kScrSrows2, kScrScols2, kScrHbuf, kScrWbest, kScrBest, kScrErr,
+    kScrGdir, kScrBlk, kScrMap, kScrWalkErr, kScrSlots
+};
+
+// Walks the path from host_state's cell through the region of `in` (until the
+// start cell or the region's top/left edge): rounds of a predicted corridor of
+// whole blocks precomputed in parallel, then walked by one warp.
+int walk_region(cudaStream_t st, int sms, const WalkInputs &in, int64_t *host_state, const Scratch &scr,
+                std::string &err, int32_t *launches);
 
 // Canonical traceback from the end cell in `out` (score, end_row, end_col set by
 // stage 1), using the stage-1 stores laid out by `plan`.  Fills out->ops,
