@@ -225,6 +225,62 @@ int swb_batch_align_device(swb_ctx *ctx, const void *d_seq, int64_t seq_bytes, c
                            swb_batch_result *out);
 void swb_batch_result_free(swb_batch_result *res);
 
+/* ---------------------------------------------------------------- serving
+ *
+ * A request loop with continuous batching.  No counterpart in the reference
+ * (one pair per process, src/main.cu:102-249).  Requests are admitted against
+ * an HBM budget for their sequences and special rows/columns.  Short requests
+ * run in iterations: each iteration batches every admitted short request into
+ * one scoring launch plus one batched traceback, and requests that arrive during
+ * an iteration join the next one.  Long requests (rows * cols above long_cells)
+ * run one at a time in a second lane on their own stream.  Their scoring grid
+ * leaves reserve_sms SMs for the short iterations, so both lanes' work overlaps
+ * on the device.  A request's result (score, end and start cells, alignment,
+ * crosspoints) is exactly what swb_align_pair() returns for the same pair. */
+
+typedef struct swb_server swb_server;
+
+typedef struct {
+    int32_t  device;
+    uint64_t hbm_budget_bytes;  /* admission budget (sequences + special rows/columns); 0 = 64 GiB */
+    int64_t  long_cells;        /* rows * cols above which a request runs in the long lane; 0 = 2^32 */
+    int32_t  max_batch;         /* most short requests per iteration; 0 = 8192                   */
+    int32_t  reserve_sms;       /* SMs kept for short iterations while a long request runs; 0 = 16 */
+    uint32_t flags;             /* SWB_FLAG_TIE_ROWMAJOR                                          */
+} swb_server_options;
+
+typedef struct {
+    double  queued_ms;          /* submit -> admission                                         */
+    double  run_ms;             /* admission -> result                                         */
+    double  total_ms;           /* submit -> result                                            */
+    int32_t lane;               /* 0 short (batched iterations), 1 long                        */
+    int32_t batch_size;         /* requests in the iteration that ran it (1 in the long lane)  */
+} swb_request_info;
+
+typedef struct {
+    int64_t submitted, completed, failed;
+    int64_t iterations;         /* short-lane iterations                                       */
+    int64_t max_batch_seen;     /* largest short iteration                                     */
+    int64_t long_completed;
+    uint64_t peak_reserved_bytes; /* largest admitted footprint at one time                   */
+    int64_t cells_completed;
+} swb_server_stats;
+
+void swb_server_options_default(swb_server_options *o);
+int swb_server_create(const swb_server_options *o, const swb_scoring *sc, swb_server **out);
+/* Copies the two sequences and queues the request; *id identifies it.  A request
+ * whose footprint exceeds the whole budget fails with SWB_ENOMEM_BUDGET here. */
+int swb_server_submit(swb_server *s, const uint8_t *a, int64_t la, const uint8_t *b, int64_t lb, uint64_t *id);
+/* Waits up to timeout_ms (< 0: forever) for request id.  SWB_OK: *out holds the
+ * result (release with swb_result_free()) and the request is forgotten;
+ * SWB_ETIMEOUT: not finished yet; SWB_ENOTFOUND: unknown id; any other code:
+ * the request failed (swb_server_last_error()) and is forgotten. */
+int swb_server_wait(swb_server *s, uint64_t id, int64_t timeout_ms, swb_result *out, swb_request_info *info);
+int swb_server_stats_get(swb_server *s, swb_server_stats *st);
+const char *swb_server_last_error(swb_server *s);
+/* Finishes the requests already admitted, drops queued ones, stops the lanes. */
+void swb_server_destroy(swb_server *s);
+
 /* Stage-1 strip trace of the context's last call when options.verbose has bit 1
  * set: per strip {start ns, end ns, SM id} from %globaltimer / %smid, written to
  * out[3*strips] (cap entries available); *count receives the strip count. */

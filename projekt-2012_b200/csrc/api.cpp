@@ -260,6 +260,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
         tab = K <= 4;
     }
     Stage1Plan plan = stage1_plan(m, n, c->sms, R, tab);
+    if (c->max_blocks > 0 && plan.blocks > c->max_blocks) plan.blocks = c->max_blocks;
     const int64_t W = (int64_t)plan.blocks * plan.warps_per_block;
     if ((e = c->hbuf.ensure(sizeof(int4) * (size_t)std::max<int64_t>(n, 1))) != cudaSuccess ||
         (e = c->wbest.ensure(sizeof(BestRec) * (size_t)W)) != cudaSuccess ||

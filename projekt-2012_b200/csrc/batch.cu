@@ -188,10 +188,12 @@ int max_blocks() {
 }
 
 template <bool TAB, class S>
-cudaError_t launch(const BatchArgs &a, int sms, cudaStream_t st) {
+cudaError_t launch(const BatchArgs &a, int sms, int cap, cudaStream_t st) {
     const int per_sm = std::max(1, max_blocks<TAB, S>());
     const int64_t need = (a.nunits + kWarps - 1) / kWarps;
-    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)per_sm * sms));
+    int64_t limit = (int64_t)per_sm * sms;
+    if (cap > 0 && cap < limit) limit = cap;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(need, limit));
     BatchArgs copy = a;
     void *args[] = {&copy};
     return cudaLaunchCooperativeKernel((const void *)batch_kernel<TAB, S>, dim3(blocks), dim3(kWarps * 32), args, 0,
@@ -205,12 +207,14 @@ int batch_max_blocks_per_sm(bool tab, bool stores) {
     return tab ? max_blocks<true, NoStores>() : max_blocks<false, NoStores>();
 }
 
-cudaError_t batch_launch(const BatchArgs &a, bool tab, bool stores, int sms, int64_t npairs, BestRec *pbest,
-                         cudaStream_t st) {
+cudaError_t batch_launch(const BatchArgs &a, bool tab, bool stores, int sms, int max_blocks, int64_t npairs,
+                         BestRec *pbest, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
     if (a.nunits > 0) {
-        if (stores) e = tab ? launch<true, WithStores>(a, sms, st) : launch<false, WithStores>(a, sms, st);
-        else e = tab ? launch<true, NoStores>(a, sms, st) : launch<false, NoStores>(a, sms, st);
+        if (stores)
+            e = tab ? launch<true, WithStores>(a, sms, max_blocks, st) : launch<false, WithStores>(a, sms, max_blocks, st);
+        else
+            e = tab ? launch<true, NoStores>(a, sms, max_blocks, st) : launch<false, NoStores>(a, sms, max_blocks, st);
         if (e != cudaSuccess) return e;
     }
     if (npairs > 0) {

@@ -51,13 +51,19 @@ constexpr int kBatchStripRows = 32 * kBatchR;
 // into pbest[slot] (which holds the pair's best so far, or an invalid record).
 // Every strip a launch runs must have its predecessor strip either earlier in the
 // same launch's unit order or finished by an earlier launch.  `stores` selects
-// the store pass.
-cudaError_t batch_launch(const BatchArgs &a, bool tab, bool stores, int sms, int64_t npairs, BestRec *pbest,
-                         cudaStream_t st);
+// the store pass.  max_blocks > 0 caps the grid (the rest of the GPU stays free
+// for other work).
+cudaError_t batch_launch(const BatchArgs &a, bool tab, bool stores, int sms, int max_blocks, int64_t npairs,
+                         BestRec *pbest, cudaStream_t st);
 // Byte presence flags over a buffer (TAB-mode choice) and the TAB encodings of
 // every byte of seq (rcode[i] = lut[seq[i]], ctab[i] = table word of seq[i]).
 cudaError_t batch_encode(const uint8_t *seq, int64_t bytes, const uint8_t *d_lut, uint8_t *rcode, uint32_t *ctab,
                          int32_t mt1, int32_t mm1, uint32_t *tab_hi, cudaStream_t st);
 int batch_max_blocks_per_sm(bool tab, bool stores);
+
+// Host batch with every pair traced, in one scoring pass that keeps the stores
+// (the serving loop's iteration).  Same contract as swb_batch_align(..., 1.0, ...).
+int batch_align_all_traced(swb_ctx *c, const uint8_t *h_seq, int64_t seq_bytes, const swb_pair_ref *pairs,
+                           int64_t npairs, const swb_scoring *sc, uint32_t flags, swb_batch_result *out);
 
 }  // namespace swb

@@ -102,7 +102,8 @@ int run_launch(swb_ctx *c, const uint8_t *d_seq, bool tab, const BatchArgs &base
         (e = cudaMemsetAsync(a.ctl, 0, 4 * sizeof(int32_t), c->stream)) != cudaSuccess)
         return ctx_cuda_fail(c, e, "batch set-up");
     cudaEventRecord(c->ev0, c->stream);
-    if ((e = batch_launch(a, tab, stores, c->sms, np, (BestRec *)c->b_pbest.p, c->stream)) != cudaSuccess)
+    if ((e = batch_launch(a, tab, stores, c->sms, c->max_blocks, np, (BestRec *)c->b_pbest.p, c->stream)) !=
+        cudaSuccess)
         return ctx_cuda_fail(c, e, "batch launch");
     cudaEventRecord(c->ev1, c->stream);
     int32_t ctl[4] = {0, 0, 0, 0};
@@ -120,8 +121,29 @@ int run_launch(swb_ctx *c, const uint8_t *d_seq, bool tab, const BatchArgs &base
     return SWB_OK;
 }
 
+// Store offsets of the traced pairs `bp` (special rows every 512 rows, special
+// columns every 256 columns) and the output capacities; returns the total
+// store entries in *srn / *scn.
+void layout_stores(std::vector<BatchPair> &bp, const swb_batch_item *items, const std::vector<int64_t> &idx,
+                   int64_t *srn, int64_t *scn, int64_t *ops_total, int64_t *xp_total) {
+    const int kBC = tb::block_cols();
+    *srn = *scn = *ops_total = *xp_total = 0;
+    for (size_t k = 0; k < bp.size(); ++k) {
+        BatchPair &d = bp[k];
+        d.sr_every = 1;
+        d.sc_every = kBC;
+        d.sr_off = *srn;
+        d.sc_off = *scn;
+        *srn += (int64_t)(d.m / kBatchStripRows) * d.n;
+        *scn += (int64_t)(d.n / kBC) * d.m;
+        *ops_total += (int64_t)d.m + d.n + 8;
+        *xp_total += d.m / items[idx[k]].xpoint_interval + 8;
+    }
+}
+
 int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t seq_bytes, const swb_pair_ref *pairs,
-              int64_t npairs, const swb_scoring *sc, uint32_t flags, double trace_frac, swb_batch_result *out) {
+              int64_t npairs, const swb_scoring *sc, uint32_t flags, double trace_frac, swb_batch_result *out,
+              bool stores_first) {
     const auto t0 = std::chrono::steady_clock::now();
     std::memset(out, 0, sizeof *out);
     if (!sc) return ctx_fail(c, SWB_EINVAL, "scoring is NULL");
@@ -216,15 +238,39 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
         }
     }
 
-    // scoring launch
+    for (int64_t i = 0; i < npairs; ++i) {
+        int32_t G = 0, T = 0;
+        int64_t P1 = 0, P2 = 0;
+        reference_geometry(info[(size_t)i].m, info[(size_t)i].n, &G, &T, &P1, &P2);
+        out->items[i].xpoint_interval = T > 0 ? 4 * T : 20;
+    }
+    auto ensure_stores = [&](int64_t srn, int64_t scn) -> int {
+        if ((uint64_t)(srn + scn) * sizeof(int2) > c->opts.hbm_budget_bytes)
+            return ctx_fail(c, SWB_ENOMEM_BUDGET, "traced pairs' special rows and columns exceed the HBM budget");
+        if ((e = c->b_srows.ensure(sizeof(int2) * (size_t)std::max<int64_t>(1, srn))) != cudaSuccess ||
+            (e = c->b_scols.ensure(sizeof(int2) * (size_t)std::max<int64_t>(1, scn))) != cudaSuccess)
+            return ctx_cuda_fail(c, e, "batch special rows and columns");
+        return SWB_OK;
+    };
+
+    // scoring launch (with the stores of every pair when all are traced anyway)
     std::vector<BatchPair> bp;
     std::vector<int32_t> unit_pair;
     std::vector<BestRec> pbest;
-    int64_t hb = 0;
+    int64_t hb = 0, srn = 0, scn = 0, ops_total = 0, xp_total = 0;
     float ms1 = 0.f;
     layout_units(info, order, flags, bp, unit_pair, &hb);
+    const bool first_stores = stores_first && !order.empty();
     if (!order.empty()) {
-        int rc = run_launch(c, d_seq, tab, base, bp, unit_pair, hb, false, pbest, &ms1);
+        BatchArgs a1 = base;
+        if (first_stores) {
+            layout_stores(bp, out->items, order, &srn, &scn, &ops_total, &xp_total);
+            int rc = ensure_stores(srn, scn);
+            if (rc != SWB_OK) return rc;
+            a1.srows = (int2 *)c->b_srows.p;
+            a1.scols = (int2 *)c->b_scols.p;
+        }
+        int rc = run_launch(c, d_seq, tab, a1, bp, unit_pair, hb, first_stores, pbest, &ms1);
         if (rc != SWB_OK) return rc;
         launches += 2;
     }
@@ -238,18 +284,14 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
         }
     }
     for (int64_t i = 0; i < npairs; ++i) {
-        swb_batch_item &it = out->items[i];
-        it.start_row = it.end_row;
-        it.start_col = it.end_col;
-        int32_t G = 0, T = 0;
-        int64_t P1 = 0, P2 = 0;
-        reference_geometry(info[(size_t)i].m, info[(size_t)i].n, &G, &T, &P1, &P2);
-        it.xpoint_interval = T > 0 ? 4 * T : 20;
+        out->items[i].start_row = out->items[i].end_row;
+        out->items[i].start_col = out->items[i].end_col;
     }
     out->stage1_ms = ms1;
 
     // traceback of the best-scoring pairs
-    const int64_t ntrace = std::min<int64_t>(npairs, (int64_t)std::ceil(trace_frac * (double)npairs - 1e-9));
+    const int64_t ntrace =
+        stores_first ? npairs : std::min<int64_t>(npairs, (int64_t)std::ceil(trace_frac * (double)npairs - 1e-9));
     if (ntrace > 0) {
         const auto t1 = std::chrono::steady_clock::now();
         std::vector<int64_t> byscore((size_t)npairs);
@@ -264,54 +306,55 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
             if (out->items[i].score > 0) tr.push_back(i);
         }
         out->n_traced = ntrace;
-        // store pass over the traced pairs: special rows every 512 rows (every
-        // strip), special columns every 256 columns
-        const int kBC = tb::block_cols();
-        std::vector<BatchPair> bp2;
-        std::vector<int32_t> up2;
-        int64_t hb2 = 0;
-        layout_units(info, tr, flags, bp2, up2, &hb2);
-        int64_t srn = 0, scn = 0, ops_total = 0, xp_total = 0;
-        for (size_t k = 0; k < tr.size(); ++k) {
-            BatchPair &d = bp2[k];
-            d.sr_every = 1;
-            d.sc_every = kBC;
-            d.sr_off = srn;
-            d.sc_off = scn;
-            srn += (int64_t)(d.m / kBatchStripRows) * d.n;
-            scn += (int64_t)(d.n / kBC) * d.m;
-            ops_total += (int64_t)d.m + d.n + 8;
-            xp_total += d.m / out->items[tr[k]].xpoint_interval + 8;
-        }
-        if ((uint64_t)(srn + scn) * sizeof(int2) > c->opts.hbm_budget_bytes)
-            return ctx_fail(c, SWB_ENOMEM_BUDGET, "traced pairs' special rows and columns exceed the HBM budget");
-        const int kS = tb::state_slots();
-        if ((e = c->b_srows.ensure(sizeof(int2) * (size_t)std::max<int64_t>(1, srn))) != cudaSuccess ||
-            (e = c->b_scols.ensure(sizeof(int2) * (size_t)std::max<int64_t>(1, scn))) != cudaSuccess ||
-            (e = c->b_ops.ensure((size_t)std::max<int64_t>(1, ops_total))) != cudaSuccess ||
-            (e = c->b_xps.ensure(sizeof(int64_t) * 4 * (size_t)std::max<int64_t>(1, xp_total))) != cudaSuccess ||
-            (e = c->b_state.ensure(sizeof(int64_t) * kS * std::max<size_t>(1, tr.size()))) != cudaSuccess ||
-            (e = c->b_walk.ensure(tb::walk_args_bytes() * std::max<size_t>(1, tr.size()))) != cudaSuccess)
-            return ctx_cuda_fail(c, e, "batch traceback buffers");
-        float ms2 = 0.f;
-        if (!tr.empty()) {
+        // the layout whose special rows and columns the walker reads, per traced pair
+        std::vector<BatchPair> bpw(tr.size());
+        if (first_stores) {
+            std::vector<int64_t> pos((size_t)npairs, -1);
+            for (size_t k = 0; k < order.size(); ++k) pos[(size_t)order[k]] = (int64_t)k;
+            for (size_t k = 0; k < tr.size(); ++k) bpw[k] = bp[(size_t)pos[(size_t)tr[k]]];
+        } else if (!tr.empty()) {
+            // store pass over the traced pairs: special rows every 512 rows (every
+            // strip), special columns every 256 columns
+            std::vector<int32_t> up2;
+            int64_t hb2 = 0;
+            layout_units(info, tr, flags, bpw, up2, &hb2);
+            layout_stores(bpw, out->items, tr, &srn, &scn, &ops_total, &xp_total);
+            int rc = ensure_stores(srn, scn);
+            if (rc != SWB_OK) return rc;
             BatchArgs b2 = base;
             b2.srows = (int2 *)c->b_srows.p;
             b2.scols = (int2 *)c->b_scols.p;
             std::vector<BestRec> pb2;
-            int rc = run_launch(c, d_seq, tab, b2, bp2, up2, hb2, true, pb2, &ms2);
+            float ms2 = 0.f;
+            rc = run_launch(c, d_seq, tab, b2, bpw, up2, hb2, true, pb2, &ms2);
             if (rc != SWB_OK) return rc;
             launches += 2;
+            for (size_t k = 0; k < tr.size(); ++k) {
+                const swb_batch_item &it = out->items[tr[k]];
+                if (!pb2[k].valid || pb2[k].ho - sc->gap_open != it.score || pb2[k].row != it.end_row ||
+                    pb2[k].col != it.end_col)
+                    return ctx_fail(c, SWB_ECUDA, "batch: store pass disagrees with the scoring pass");
+            }
+        }
+        if (!tr.empty()) {
+            ops_total = xp_total = 0;
+            for (size_t k = 0; k < tr.size(); ++k) {
+                ops_total += (int64_t)bpw[k].m + bpw[k].n + 8;
+                xp_total += bpw[k].m / out->items[tr[k]].xpoint_interval + 8;
+            }
+            const int kS = tb::state_slots();
+            if ((e = c->b_ops.ensure((size_t)std::max<int64_t>(1, ops_total))) != cudaSuccess ||
+                (e = c->b_xps.ensure(sizeof(int64_t) * 4 * (size_t)std::max<int64_t>(1, xp_total))) != cudaSuccess ||
+                (e = c->b_state.ensure(sizeof(int64_t) * kS * std::max<size_t>(1, tr.size()))) != cudaSuccess ||
+                (e = c->b_walk.ensure(tb::walk_args_bytes() * std::max<size_t>(1, tr.size()))) != cudaSuccess)
+                return ctx_cuda_fail(c, e, "batch traceback buffers");
             std::vector<tb::WalkInputs> win(tr.size());
             std::vector<int64_t> st((size_t)kS * tr.size(), 0);
             int64_t oo = 0, xo = 0;
             std::vector<int64_t> ops_off(tr.size()), xp_off(tr.size());
             for (size_t k = 0; k < tr.size(); ++k) {
                 const swb_batch_item &it = out->items[tr[k]];
-                const BatchPair &d = bp2[k];
-                const BestRec &b = pb2[k];
-                if (!b.valid || b.ho - sc->gap_open != it.score || b.row != it.end_row || b.col != it.end_col)
-                    return ctx_fail(c, SWB_ECUDA, "batch: store pass disagrees with the scoring pass");
+                const BatchPair &d = bpw[k];
                 tb::WalkInputs &w = win[k];
                 w.rows = d_seq + d.row_off;
                 w.cols = d_seq + d.col_off;
@@ -342,8 +385,8 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
                 S[tb::slot_c()] = it.end_col;
             }
             std::string err;
-            rc = tb::walk_batch(c->stream, c->sms, win.data(), (int64_t)win.size(), c->b_walk.p,
-                                (int64_t *)c->b_state.p, st.data(), err);
+            int rc = tb::walk_batch(c->stream, c->sms, win.data(), (int64_t)win.size(), c->b_walk.p,
+                                    (int64_t *)c->b_state.p, st.data(), err);
             if (rc != SWB_OK) return ctx_fail(c, rc, "%s", err.c_str());
             launches += 1;
             // gather: ops (end -> start on the device) and crosspoints
@@ -391,9 +434,10 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
             out->n_xpoints = px;
         }
         // traced pairs with score 0: no alignment; crosspoints [start = end]
+        // (pairs with an empty sequence have none, as in swb_align_pair)
         for (int64_t i : byscore) {
             swb_batch_item &it = out->items[i];
-            if (it.score > 0) continue;
+            if (it.score > 0 || info[(size_t)i].n == 0) continue;
             if (!out->xpoints) {
                 out->xpoints = (swb_xpoint *)std::malloc(sizeof(swb_xpoint) * (size_t)(ntrace + 1));
                 if (!out->xpoints) return ctx_fail(c, SWB_ENOMEM, "out of host memory");
@@ -410,13 +454,21 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
 }
 
 }  // namespace
+
+int batch_align_all_traced(swb_ctx *c, const uint8_t *h_seq, int64_t seq_bytes, const swb_pair_ref *pairs,
+                           int64_t npairs, const swb_scoring *sc, uint32_t flags, swb_batch_result *out) {
+    int rc = batch_run(c, h_seq, nullptr, seq_bytes, pairs, npairs, sc, flags, 1.0, out, true);
+    if (rc != SWB_OK) swb_batch_result_free(out);
+    return rc;
+}
+
 }  // namespace swb
 
 extern "C" int swb_batch_align(swb_ctx *c, const uint8_t *seq, int64_t seq_bytes, const swb_pair_ref *pairs,
                                int64_t npairs, const swb_scoring *sc, uint32_t flags, double trace_frac,
                                swb_batch_result *out) {
     if (!c || !out || (seq_bytes > 0 && !seq)) return swb::ctx_fail(c, SWB_EINVAL, "swb_batch_align: bad arguments");
-    int rc = swb::batch_run(c, seq, nullptr, seq_bytes, pairs, npairs, sc, flags, trace_frac, out);
+    int rc = swb::batch_run(c, seq, nullptr, seq_bytes, pairs, npairs, sc, flags, trace_frac, out, trace_frac >= 1.0);
     if (rc != SWB_OK) swb_batch_result_free(out);
     return rc;
 }
@@ -426,7 +478,8 @@ extern "C" int swb_batch_align_device(swb_ctx *c, const void *d_seq, int64_t seq
                                       swb_batch_result *out) {
     if (!c || !out || (seq_bytes > 0 && !d_seq))
         return swb::ctx_fail(c, SWB_EINVAL, "swb_batch_align_device: bad arguments");
-    int rc = swb::batch_run(c, nullptr, (const uint8_t *)d_seq, seq_bytes, pairs, npairs, sc, flags, trace_frac, out);
+    int rc = swb::batch_run(c, nullptr, (const uint8_t *)d_seq, seq_bytes, pairs, npairs, sc, flags, trace_frac, out,
+                            trace_frac >= 1.0);
     if (rc != SWB_OK) swb_batch_result_free(out);
     return rc;
 }

@@ -48,6 +48,7 @@ struct swb_ctx {
     // last stage-1 special-row layout (for swb_special_row_copy)
     int64_t last_nsr = 0, last_n = 0, last_sr_interval = 0;
     int32_t last_launches = 0;  // this library's kernels launched by the last stage 1
+    int32_t max_blocks = 0;     // cap on the scoring grids of this context (0 = whole GPU); set by the server
 };
 
 namespace swb {

@@ -74,6 +74,22 @@ class BatchResult(C.Structure):
                 ("kernel_launches", C.c_int32)]
 
 
+class ServerOptions(C.Structure):
+    _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64), ("long_cells", C.c_int64),
+                ("max_batch", C.c_int32), ("reserve_sms", C.c_int32), ("flags", C.c_uint32)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("queued_ms", C.c_double), ("run_ms", C.c_double), ("total_ms", C.c_double),
+                ("lane", C.c_int32), ("batch_size", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
+                ("iterations", C.c_int64), ("max_batch_seen", C.c_int64), ("long_completed", C.c_int64),
+                ("peak_reserved_bytes", C.c_uint64), ("cells_completed", C.c_int64)]
+
+
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64),
                 ("special_interval", C.c_int32), ("verbose", C.c_int32),
@@ -126,6 +142,20 @@ def lib():
         L.swb_batch_align_device.argtypes = L.swb_batch_align.argtypes
         L.swb_batch_align_device.restype = C.c_int
         L.swb_batch_result_free.argtypes = [C.POINTER(BatchResult)]
+        L.swb_server_options_default.argtypes = [C.POINTER(ServerOptions)]
+        L.swb_server_create.argtypes = [C.POINTER(ServerOptions), C.POINTER(Scoring), C.POINTER(C.c_void_p)]
+        L.swb_server_create.restype = C.c_int
+        L.swb_server_submit.argtypes = [C.c_void_p, C.c_char_p, C.c_int64, C.c_char_p, C.c_int64,
+                                        C.POINTER(C.c_uint64)]
+        L.swb_server_submit.restype = C.c_int
+        L.swb_server_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_int64, C.POINTER(Result),
+                                      C.POINTER(RequestInfo)]
+        L.swb_server_wait.restype = C.c_int
+        L.swb_server_stats_get.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
+        L.swb_server_stats_get.restype = C.c_int
+        L.swb_server_last_error.argtypes = [C.c_void_p]
+        L.swb_server_last_error.restype = C.c_char_p
+        L.swb_server_destroy.argtypes = [C.c_void_p]
         L.swb_probe_cell_peak.argtypes = [C.c_int32] + [C.POINTER(C.c_double)] * 5
         L.swb_probe_cell_peak.restype = C.c_int
         L.swb_probe_latency.argtypes = [C.c_int32, C.POINTER(C.c_double), C.c_int32]
@@ -384,3 +414,67 @@ def probe_latency(device: int = 0) -> dict:
         raise SwbError(rc, "latency probe failed")
     names = ["iadd", "max_add_c", "viaddmax", "vimax3", "viaddmax_relu", "max_c"]
     return dict(zip(names, list(v)))
+
+
+class Server:
+    """The serving loop (swb_server_*): submit requests at any time, wait for
+    each one's result; short requests are batched per iteration, long ones run
+    in a second lane beside them."""
+
+    def __init__(self, sc: Scoring, device: int = 0, hbm_budget_bytes: int = 0, long_cells: int = 0,
+                 max_batch: int = 0, reserve_sms: int = 0, flags: int = 0):
+        L = lib()
+        o = ServerOptions()
+        L.swb_server_options_default(C.byref(o))
+        o.device, o.hbm_budget_bytes, o.long_cells = device, hbm_budget_bytes, long_cells
+        o.max_batch, o.reserve_sms, o.flags = max_batch, reserve_sms, flags
+        h = C.c_void_p()
+        self._sc = Scoring(sc.match, sc.mismatch, sc.gap_open, sc.gap_extend)
+        rc = L.swb_server_create(C.byref(o), C.byref(self._sc), C.byref(h))
+        if rc != SWB_OK:
+            raise SwbError(rc, L.swb_last_error(None).decode())
+        self._h = h
+
+    def submit(self, a: bytes, b: bytes) -> int:
+        rid = C.c_uint64(0)
+        rc = lib().swb_server_submit(self._h, a, len(a), b, len(b), C.byref(rid))
+        if rc != SWB_OK:
+            raise SwbError(rc, lib().swb_last_error(None).decode())
+        return rid.value
+
+    def wait(self, rid: int, timeout_ms: int = -1):
+        """(Alignment, info dict) or None when timeout_ms ran out."""
+        r, info = Result(), RequestInfo()
+        L = lib()
+        rc = L.swb_server_wait(self._h, rid, timeout_ms, C.byref(r), C.byref(info))
+        if rc == SWB_ETIMEOUT:
+            return None
+        if rc != SWB_OK:
+            raise SwbError(rc, (L.swb_server_last_error(self._h) or b"").decode())
+        try:
+            return _convert(r), {"queued_ms": info.queued_ms, "run_ms": info.run_ms, "total_ms": info.total_ms,
+                                 "lane": info.lane, "batch_size": info.batch_size}
+        finally:
+            L.swb_result_free(C.byref(r))
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        lib().swb_server_stats_get(self._h, C.byref(st))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().swb_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
