@@ -38,6 +38,9 @@ def parse_args():
                    default="long")
     p.add_argument("--score-only", action="store_true", help="stage 1 only (diagnostics)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-mixed", action="store_true", help="skip the batched and serving measurements")
+    p.add_argument("--batch-pairs", type=int, default=100_000, help="pairs of the batched workload")
+    p.add_argument("--serve-seconds", type=float, default=20.0, help="length of the Poisson serving run")
     return p.parse_args()
 
 
@@ -200,6 +203,135 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def percentile(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = min(len(xs) - 1, max(0, int(round(q / 100.0 * (len(xs) - 1)))))
+    return xs[k]
+
+
+def batched_metrics(args, device):
+    """The batched workload (100,000 pairs, log-normal query lengths, 1% traced)
+    through swb_batch_align from a host buffer (copies inside the timed region),
+    against the plain pair path (swb_align_pair, score only) on a sample of the
+    same pairs."""
+    import numpy as np
+    import swb200
+    from swb200 import synth
+    buf, refs, sc_t = synth.batched(args.batch_pairs)
+    sc = swb200.scoring(*sc_t)
+    ctx = swb200.Context(device=device)
+    for _ in range(2):
+        ctx.batch_align(buf, refs, sc, trace_frac=0.01)
+    runs = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        r = ctx.batch_align(buf, refs, sc, trace_frac=0.01)
+        runs.append((time.perf_counter() - t0, r.stage1_ms, r.stage2_ms, r.kernel_launches))
+    wall = min(x[0] for x in runs)
+    rng = np.random.default_rng(0)
+    sample = rng.choice(len(refs), size=min(400, len(refs)), replace=False)
+    t0 = time.perf_counter()
+    for i in sample:
+        ao, al, bo, bl = (int(v) for v in refs[i])
+        p = ctx.align(buf[ao:ao + al].tobytes(), buf[bo:bo + bl].tobytes(), sc, swb200.FLAG_SCORE_ONLY)
+        assert (p.score, p.end_row, p.end_col) == (r.score[i], r.end_row[i], r.end_col[i])
+    plain = len(sample) / (time.perf_counter() - t0)
+    ctx.close()
+    n = len(refs)
+    return {"workload": f"{n} pairs, query clip(round(lognormal(ln 1000, 0.75)), 100, 10000), target 1.5x "
+                        "(8% sub, 1% indel); scoring 2/-3/-5/-2; score + end cell of every pair, alignment of "
+                        "the best 1%",
+            "pairs_per_s": n / wall, "gcups": r.cells / wall / 1e9, "ms_per_batch": wall * 1e3,
+            "stage1_ms": min(x[1] for x in runs), "stage2_ms": min(x[2] for x in runs),
+            "kernel_launches": runs[-1][3], "plain_pairs_per_s": plain, "vs_plain": n / wall / plain,
+            "plain_sample": f"{len(sample)} pairs of the same batch through swb_align_pair, score only, equal results",
+            "timing": "wall clock of swb_batch_align from host memory (host->device copy, results back)"}
+
+
+def serving_metrics(args, device):
+    """Poisson stream of the serving mix at 80% of the measured capacity through
+    the serving loop (swb_server_*), with latency per request; the plain path's
+    latency for the same arrivals is a FIFO queue served one pair at a time by
+    swb_align_pair, with service times measured on a sample."""
+    import numpy as np
+    import swb200
+    from swb200 import synth
+    sc_t = (1, -3, -5, -2)
+    sc = swb200.scoring(*sc_t)
+    budget = 100 << 30
+    # capacity: a burst from an independent draw of the same mix
+    cap_rng = synth.rng_for(4, 99)
+    burst = [synth.serving_request(cap_rng) for _ in range(160)]
+    with swb200.Server(sc, device=device, hbm_budget_bytes=budget) as srv:
+        t0 = time.perf_counter()
+        ids = [srv.submit(q, t) for q, t, _ in burst]
+        for i in ids:
+            srv.wait(i)
+        cap_t = time.perf_counter() - t0
+    capacity = len(burst) / cap_t
+    rate = 0.8 * capacity
+    stream = synth.serving_stream(args.serve_seconds, rate)
+    lat, lanes, cells = [], [], 0
+    with swb200.Server(sc, device=device, hbm_budget_bytes=budget) as srv:
+        ids = []
+        start = time.perf_counter()
+        for t_arr, q, tg, _ in stream:
+            now = time.perf_counter() - start
+            if t_arr > now:
+                time.sleep(t_arr - now)
+            ids.append(srv.submit(q, tg))
+        for (t_arr, q, tg, lg), i in zip(stream, ids):
+            res, info = srv.wait(i)
+            lat.append(info["total_ms"])
+            lanes.append(info["lane"])
+            cells += len(q) * len(tg)
+        span = time.perf_counter() - start
+        st = srv.stats()
+    # plain path: service times on a sample, FIFO over the same arrivals
+    ctx = swb200.Context(device=device, hbm_budget_bytes=budget // 2)
+    short = [(q, tg) for _, q, tg, lg in stream if not lg][:200]
+    longs = [(q, tg) for _, q, tg, lg in stream if lg][:2]
+    svc_short = []
+    for q, tg in short:
+        t0 = time.perf_counter()
+        ctx.align(q, tg, sc)
+        svc_short.append(time.perf_counter() - t0)
+    long_rate = None
+    if longs:
+        tt, cc = 0.0, 0
+        for q, tg in longs:
+            t0 = time.perf_counter()
+            ctx.align(q, tg, sc)
+            tt += time.perf_counter() - t0
+            cc += len(q) * len(tg)
+        long_rate = cc / tt
+    ctx.close()
+    mean_short = float(np.mean(svc_short)) if svc_short else 0.0
+    clock, plain_lat = 0.0, []
+    for t_arr, q, tg, lg in stream:
+        svc = (len(q) * len(tg) / long_rate) if (lg and long_rate) else mean_short
+        clock = max(clock, t_arr) + svc
+        plain_lat.append((clock - t_arr) * 1e3)
+    short_lat = [x for x, l in zip(lat, lanes) if l == 0]
+    long_lat = [x for x, l in zip(lat, lanes) if l == 1]
+    return {"workload": f"Poisson arrivals for {args.serve_seconds:g} s at 80% of measured capacity; 95% short "
+                        "(query U[200, 5000], target 1.5x, 7% sub + 1% indel), 5% long (query U[100k, 2M], target "
+                        "1.5x, 2.5% sub + 0.5% indel); scoring 1/-3/-5/-2; full traceback; HBM budget 100 GiB",
+            "capacity_pairs_per_s": capacity, "arrival_rate": rate, "requests": len(stream),
+            "long_requests": int(sum(lanes)), "pairs_per_s": len(stream) / span, "gcups": cells / span / 1e9,
+            "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99),
+            "short_p50_ms": percentile(short_lat, 50), "short_p99_ms": percentile(short_lat, 99),
+            "long_p50_ms": percentile(long_lat, 50), "long_p99_ms": percentile(long_lat, 99),
+            "iterations": st["iterations"], "max_batch": st["max_batch_seen"],
+            "plain_fifo_p50_ms": percentile(plain_lat, 50), "plain_fifo_p99_ms": percentile(plain_lat, 99),
+            "plain_pairs_per_s": len(stream) / max(clock, args.serve_seconds),
+            "plain_model": f"FIFO, one pair at a time through swb_align_pair: short service {mean_short * 1e3:.2f} ms "
+                           f"(mean of {len(svc_short)} measured), long service = cells / "
+                           f"{(long_rate or 0) / 1e9:.0f} GCUPS (measured on {len(longs)} long requests)"}
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -284,6 +416,11 @@ def main():
             dist.destroy_process_group()
         return
     cpu = None if args.no_cpu_baseline else cpu_baseline(a, b, sc_t)
+    mixed_batched = mixed_serving = None
+    if not args.no_mixed:
+        ctx.close()
+        mixed_batched = batched_metrics(args, local)
+        mixed_serving = serving_metrics(args, local)
     d2h = 64 + first.n_ops + 24 * len(first.xpoints)
     line = {
         "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
@@ -305,6 +442,8 @@ def main():
         "e2e": {"value": e2e, "unit": "GCUPS", "h2d_bytes_per_step": len(a) + len(b),
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
+        "batched": mixed_batched,
+        "serving": mixed_serving,
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)

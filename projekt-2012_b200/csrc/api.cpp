@@ -28,17 +28,18 @@ namespace swb {
 
 cudaError_t DevBuf::ensure(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, st);
     p = nullptr;
     cap = 0;
     size_t want = bytes < 256 ? 256 : bytes;
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = cudaMallocAsync(&p, want, st);
     if (e == cudaSuccess) cap = want;
+    else p = nullptr;
     return e;
 }
 
 void DevBuf::release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, st);
     p = nullptr;
     cap = 0;
 }
@@ -73,6 +74,26 @@ int ctx_fail(swb_ctx *ctx, int code, const char *fmt, ...) {
 
 int ctx_cuda_fail(swb_ctx *ctx, cudaError_t e, const char *what) {
     return ctx_fail(ctx, SWB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+cudaError_t ctx_get(swb_ctx *c, void *dst, const void *dev_src, size_t bytes) {
+    if (bytes == 0) return cudaSuccess;
+    cudaError_t e;
+    if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess || (e = c->h_io.ensure(bytes)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(c->h_io.p, dev_src, bytes, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+        return e;
+    std::memcpy(dst, c->h_io.p, bytes);
+    return cudaSuccess;
+}
+
+cudaError_t ctx_put(swb_ctx *c, void *dev_dst, const void *src, size_t bytes) {
+    if (bytes == 0) return cudaSuccess;
+    cudaError_t e;
+    if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess || (e = c->h_io.ensure(bytes)) != cudaSuccess)
+        return e;
+    std::memcpy(c->h_io.p, src, bytes);
+    return cudaMemcpyAsync(dev_dst, c->h_io.p, bytes, cudaMemcpyHostToDevice, c->stream);
 }
 
 }  // namespace swb
@@ -141,7 +162,9 @@ int swb_ctx_create(const swb_options *opts, swb_ctx **out) {
         (e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device)) != cudaSuccess ||
         (c->opts.cuda_stream == 0 &&
          (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) ||
-        (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess) {
+        (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess ||
+        (e = swb::stage1_configure()) != cudaSuccess || (e = swb::batch_configure()) != cudaSuccess ||
+        (e = swb::tb::walker_configure()) != cudaSuccess) {
         int rc = ctx_cuda_fail(nullptr, e, "swb_ctx_create");
         delete c;
         return rc;
@@ -150,6 +173,7 @@ int swb_ctx_create(const swb_options *opts, swb_ctx **out) {
         c->stream = (cudaStream_t)(uintptr_t)c->opts.cuda_stream;
         c->own_stream = false;
     }
+    c->each_buf([c](DevBuf &b) { b.st = c->stream; });
     *out = c;
     return SWB_OK;
 }
@@ -158,15 +182,10 @@ void swb_ctx_destroy(swb_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (DevBuf *b : {&c->rows, &c->cols, &c->hbuf, &c->wbest, &c->best, &c->errf, &c->srows, &c->scols,
-                      &c->work, &c->flags, &c->lut, &c->rcode, &c->ctab, &c->trace})
-        b->release();
-    for (DevBuf &b : c->tb) b.release();
-    for (DevBuf *b : {&c->b_seq, &c->b_rcode, &c->b_ctab, &c->b_pairs, &c->b_units, &c->b_hbuf, &c->b_gbest,
-                      &c->b_ubest, &c->b_pbest, &c->b_ctl, &c->b_srows, &c->b_scols, &c->b_walk, &c->b_ops,
-                      &c->b_xps, &c->b_state})
-        b->release();
+    c->each_buf([](DevBuf &b) { b.release(); });
+    if (c->stream) cudaStreamSynchronize(c->stream);
     c->h_stage.release();
+    c->h_io.release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
@@ -250,9 +269,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
         uint32_t present[256];
         if ((e = c->flags.ensure(256 * sizeof(uint32_t))) != cudaSuccess ||
             (e = stage1_presence(d_cols, n, (uint32_t *)c->flags.p, c->stream)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(present, c->flags.p, sizeof present, cudaMemcpyDeviceToHost, c->stream)) !=
-                cudaSuccess ||
-            (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+            (e = swb::ctx_get(c, present, c->flags.p, sizeof present)) != cudaSuccess)
             return ctx_cuda_fail(c, e, "column alphabet");
         c->last_launches += 1;
         int K = 0;
@@ -281,7 +298,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     if (tab) {
         if ((e = c->lut.ensure(256)) != cudaSuccess || (e = c->rcode.ensure((size_t)m + 64)) != cudaSuccess ||
             (e = c->ctab.ensure(sizeof(uint32_t) * ((size_t)n + 64))) != cudaSuccess ||
-            (e = cudaMemcpyAsync(c->lut.p, lut, 256, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+            (e = swb::ctx_put(c, c->lut.p, lut, 256)) != cudaSuccess ||
             (e = stage1_encode(d_rows, m, d_cols, n, (const uint8_t *)c->lut.p, (uint8_t *)c->rcode.p,
                                (uint32_t *)c->ctab.p, mt1, mm1, &a.tab_hi, c->stream)) != cudaSuccess)
             return ctx_cuda_fail(c, e, "stage 1 encode");
@@ -358,9 +375,8 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     if ((e = stage1_launch(a, plan, c->stream)) != cudaSuccess) return ctx_cuda_fail(c, e, "stage 1 launch");
     cudaEventRecord(c->ev1, c->stream);
     int32_t errh[2] = {0, 0};
-    if ((e = cudaMemcpyAsync(best_out, a.best, sizeof(BestRec), cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(errh, a.err, sizeof errh, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+    if ((e = swb::ctx_get(c, best_out, a.best, sizeof(BestRec))) != cudaSuccess ||
+        (e = swb::ctx_get(c, errh, a.err, sizeof errh)) != cudaSuccess)
         return ctx_cuda_fail(c, e, "stage 1");
     if (errh[0] != 0) return ctx_fail(c, SWB_ETIMEOUT, "stage 1: a bounded wait between strips ran out");
     float ms = 0.f;
@@ -423,6 +439,12 @@ int align_device(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_
             swb_ctx *cx = (swb_ctx *)owner;
             return cx->tb[which].ensure(bytes) == cudaSuccess ? cx->tb[which].p : nullptr;
         };
+        scr.get = [](void *owner, void *dst, const void *src, size_t bytes) -> cudaError_t {
+            return swb::ctx_get((swb_ctx *)owner, dst, src, bytes);
+        };
+        scr.put = [](void *owner, void *dst, const void *src, size_t bytes) -> cudaError_t {
+            return swb::ctx_put((swb_ctx *)owner, dst, src, bytes);
+        };
         int32_t launches = 0;
         rc = tb::traceback(c->stream, c->sms, d_rows, m, d_cols, n, sc, plan, (const int2 *)c->srows.p,
                            (const int2 *)c->scols.p, out, scr, c->err, &launches);
@@ -473,10 +495,8 @@ extern "C" int swb_align_pair(swb_ctx *c, const uint8_t *a, int64_t la, const ui
     cudaError_t e;
     if ((e = c->rows.ensure((size_t)m + 64)) != cudaSuccess || (e = c->cols.ensure((size_t)n + 64)) != cudaSuccess)
         return ctx_cuda_fail(c, e, "sequence buffers");
-    if (m > 0 && (e = cudaMemcpyAsync(c->rows.p, hr, (size_t)m, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
-        return ctx_cuda_fail(c, e, "copy rows");
-    if (n > 0 && (e = cudaMemcpyAsync(c->cols.p, hc, (size_t)n, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
-        return ctx_cuda_fail(c, e, "copy cols");
+    if ((e = swb::ctx_put(c, c->rows.p, hr, (size_t)m)) != cudaSuccess) return ctx_cuda_fail(c, e, "copy rows");
+    if ((e = swb::ctx_put(c, c->cols.p, hc, (size_t)n)) != cudaSuccess) return ctx_cuda_fail(c, e, "copy cols");
     return align_device(c, (const uint8_t *)c->rows.p, m, (const uint8_t *)c->cols.p, n, sc, flags, out, swap ? 1 : 0);
 }
 
@@ -488,8 +508,7 @@ extern "C" int swb_special_row_copy(swb_ctx *c, int64_t idx, int32_t *out, int64
     if (idx < 0 || idx >= c->last_nsr || cols != c->last_n)
         return ctx_fail(c, SWB_EINVAL, "special row %lld not available", (long long)idx);
     cudaSetDevice(c->device);
-    cudaError_t e = cudaMemcpy(out, (const int2 *)c->srows.p + idx * c->last_n, sizeof(int2) * (size_t)cols,
-                               cudaMemcpyDeviceToHost);
+    cudaError_t e = swb::ctx_get(c, out, (const int2 *)c->srows.p + idx * c->last_n, sizeof(int2) * (size_t)cols);
     if (e != cudaSuccess) return ctx_cuda_fail(c, e, "special row copy");
     return SWB_OK;
 }
@@ -501,6 +520,6 @@ extern "C" int swb_trace_copy(swb_ctx *c, int64_t *out, int64_t cap, int64_t *co
     *count = c->last_nstrips;
     if (!c->trace.p || cap < 3 * c->last_nstrips) return ctx_fail(c, SWB_EINVAL, "no trace or buffer too small");
     cudaSetDevice(c->device);
-    cudaError_t e = cudaMemcpy(out, c->trace.p, sizeof(int64_t) * 3 * (size_t)c->last_nstrips, cudaMemcpyDeviceToHost);
+    cudaError_t e = swb::ctx_get(c, out, c->trace.p, sizeof(int64_t) * 3 * (size_t)c->last_nstrips);
     return e == cudaSuccess ? SWB_OK : ctx_cuda_fail(c, e, "trace copy");
 }

@@ -10,8 +10,8 @@
 // per lane).  The host lists every strip of every pair as one work unit, pair
 // after pair (longest pairs first, each pair's strips in order), and warps claim
 // units from a device counter.  A unit's only dependency is the strip above it,
-// which was claimed earlier by a warp that is resident (the launch is
-// cooperative), so every wait ends.  A short pair (<= 512 rows) is one unit: one
+// which an earlier claim gave to a warp that is already running, so every wait
+// ends whether or not the whole grid is resident at once.  A short pair (<= 512 rows) is one unit: one
 // warp aligns it alone (inter-sequence mapping).  A longer pair's strips run on
 // consecutive warps that pass the strip's bottom row down through the pair's
 // tagged row buffer as in the single-pair kernel (intra-sequence wavefront).
@@ -194,13 +194,25 @@ cudaError_t launch(const BatchArgs &a, int sms, int cap, cudaStream_t st) {
     int64_t limit = (int64_t)per_sm * sms;
     if (cap > 0 && cap < limit) limit = cap;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(need, limit));
-    BatchArgs copy = a;
-    void *args[] = {&copy};
-    return cudaLaunchCooperativeKernel((const void *)batch_kernel<TAB, S>, dim3(blocks), dim3(kWarps * 32), args, 0,
-                                       st);
+    batch_kernel<TAB, S><<<blocks, kWarps * 32, 0, st>>>(a);
+    return cudaGetLastError();
 }
 
 }  // namespace
+
+cudaError_t batch_configure() {
+    const int c = cudaSharedmemCarveoutMaxShared;
+    const auto A = cudaFuncAttributePreferredSharedMemoryCarveout;
+    cudaError_t e = cudaSuccess;
+    for (cudaError_t x : {cudaFuncSetAttribute((const void *)batch_kernel<false, NoStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_kernel<true, NoStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_kernel<false, WithStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_kernel<true, WithStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_reduce_kernel, A, c),
+                          cudaFuncSetAttribute((const void *)batch_encode_kernel, A, c)})
+        if (x != cudaSuccess) e = x;
+    return e;
+}
 
 int batch_max_blocks_per_sm(bool tab, bool stores) {
     if (stores) return tab ? max_blocks<true, WithStores>() : max_blocks<false, WithStores>();

@@ -77,7 +77,7 @@ int run_launch(swb_ctx *c, const uint8_t *d_seq, bool tab, const BatchArgs &base
         (e = c->b_ubest.ensure(sizeof(BestRec) * (size_t)std::max<int64_t>(1, nu))) != cudaSuccess ||
         (e = c->b_pbest.ensure(sizeof(BestRec) * (size_t)np)) != cudaSuccess ||
         (e = c->b_ctl.ensure(4 * sizeof(int32_t))) != cudaSuccess ||
-        (e = c->h_stage.ensure(std::max(bp_bytes + up_bytes, sizeof(BestRec) * (size_t)np) + 64)) != cudaSuccess)
+        (e = c->h_stage.ensure(std::max(bp_bytes + up_bytes, sizeof(BestRec) * (size_t)np + 64) + 64)) != cudaSuccess)
         return ctx_cuda_fail(c, e, "batch buffers");
     // descriptors through pinned staging (one buffer, two copies)
     uint8_t *hs = (uint8_t *)c->h_stage.p;
@@ -108,11 +108,13 @@ int run_launch(swb_ctx *c, const uint8_t *d_seq, bool tab, const BatchArgs &base
     cudaEventRecord(c->ev1, c->stream);
     int32_t ctl[4] = {0, 0, 0, 0};
     pbest.resize((size_t)np);
+    int32_t *hctl = (int32_t *)(hs + sizeof(BestRec) * (size_t)np);  // pinned, after the records
     if ((e = cudaMemcpyAsync(hs, c->b_pbest.p, sizeof(BestRec) * (size_t)np, cudaMemcpyDeviceToHost, c->stream)) !=
             cudaSuccess ||
-        (e = cudaMemcpyAsync(ctl, a.ctl, sizeof ctl, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(hctl, a.ctl, sizeof ctl, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
         return ctx_cuda_fail(c, e, "batch");
+    std::memcpy(ctl, hctl, sizeof ctl);
     if (ctl[1] != 0) return ctx_fail(c, SWB_ETIMEOUT, "batch: a bounded wait between strips ran out");
     std::memcpy(pbest.data(), hs, sizeof(BestRec) * (size_t)np);
     float t = 0.f;
@@ -188,9 +190,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
     const uint8_t *d_seq = d_seq_in;
     if (h_seq) {
         if ((e = c->b_seq.ensure((size_t)seq_bytes + 64)) != cudaSuccess) return ctx_cuda_fail(c, e, "batch sequences");
-        if (seq_bytes > 0 &&
-            (e = cudaMemcpyAsync(c->b_seq.p, h_seq, (size_t)seq_bytes, cudaMemcpyHostToDevice, c->stream)) !=
-                cudaSuccess)
+        if ((e = ctx_put(c, c->b_seq.p, h_seq, (size_t)seq_bytes)) != cudaSuccess)
             return ctx_cuda_fail(c, e, "copy batch sequences");
         d_seq = (const uint8_t *)c->b_seq.p;
     }
@@ -216,9 +216,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
         uint32_t present[256];
         if ((e = c->flags.ensure(256 * sizeof(uint32_t))) != cudaSuccess ||
             (e = stage1_presence(d_seq, seq_bytes, (uint32_t *)c->flags.p, c->stream)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(present, c->flags.p, sizeof present, cudaMemcpyDeviceToHost, c->stream)) !=
-                cudaSuccess ||
-            (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+            (e = ctx_get(c, present, c->flags.p, sizeof present)) != cudaSuccess)
             return ctx_cuda_fail(c, e, "batch alphabet");
         launches += 1;
         uint8_t lut[256];
@@ -228,7 +226,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
             tab = true;
             if ((e = c->lut.ensure(256)) != cudaSuccess || (e = c->b_rcode.ensure((size_t)seq_bytes + 64)) != cudaSuccess ||
                 (e = c->b_ctab.ensure(sizeof(uint32_t) * ((size_t)seq_bytes + 64))) != cudaSuccess ||
-                (e = cudaMemcpyAsync(c->lut.p, lut, 256, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+                (e = ctx_put(c, c->lut.p, lut, 256)) != cudaSuccess ||
                 (e = batch_encode(d_seq, seq_bytes, (const uint8_t *)c->lut.p, (uint8_t *)c->b_rcode.p,
                                   (uint32_t *)c->b_ctab.p, base.mt1, base.mm1, &base.tab_hi, c->stream)) != cudaSuccess)
                 return ctx_cuda_fail(c, e, "batch encode");
@@ -346,7 +344,8 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
             if ((e = c->b_ops.ensure((size_t)std::max<int64_t>(1, ops_total))) != cudaSuccess ||
                 (e = c->b_xps.ensure(sizeof(int64_t) * 4 * (size_t)std::max<int64_t>(1, xp_total))) != cudaSuccess ||
                 (e = c->b_state.ensure(sizeof(int64_t) * kS * std::max<size_t>(1, tr.size()))) != cudaSuccess ||
-                (e = c->b_walk.ensure(tb::walk_args_bytes() * std::max<size_t>(1, tr.size()))) != cudaSuccess)
+                (e = c->b_walk.ensure(tb::walk_args_bytes() * std::max<size_t>(1, tr.size()))) != cudaSuccess ||
+                (e = c->b_gdir.ensure(tb::walk_batch_dir_bytes(c->sms, (int64_t)tr.size()))) != cudaSuccess)
                 return ctx_cuda_fail(c, e, "batch traceback buffers");
             std::vector<tb::WalkInputs> win(tr.size());
             std::vector<int64_t> st((size_t)kS * tr.size(), 0);
@@ -385,8 +384,16 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
                 S[tb::slot_c()] = it.end_col;
             }
             std::string err;
+            tb::Scratch scr{};
+            scr.owner = c;
+            scr.get = [](void *owner, void *dst, const void *src, size_t bytes) -> cudaError_t {
+                return ctx_get((swb_ctx *)owner, dst, src, bytes);
+            };
+            scr.put = [](void *owner, void *dst, const void *src, size_t bytes) -> cudaError_t {
+                return ctx_put((swb_ctx *)owner, dst, src, bytes);
+            };
             int rc = tb::walk_batch(c->stream, c->sms, win.data(), (int64_t)win.size(), c->b_walk.p,
-                                    (int64_t *)c->b_state.p, st.data(), err);
+                                    (int64_t *)c->b_state.p, c->b_gdir.p, st.data(), scr, err);
             if (rc != SWB_OK) return ctx_fail(c, rc, "%s", err.c_str());
             launches += 1;
             // gather: ops (end -> start on the device) and crosspoints
@@ -400,11 +407,8 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
             }
             std::vector<char> hops((size_t)std::max<int64_t>(1, oo));
             std::vector<int64_t> hxp((size_t)std::max<int64_t>(4, 4 * xo));
-            if ((e = cudaMemcpyAsync(hops.data(), c->b_ops.p, (size_t)oo, cudaMemcpyDeviceToHost, c->stream)) !=
-                    cudaSuccess ||
-                (e = cudaMemcpyAsync(hxp.data(), c->b_xps.p, sizeof(int64_t) * 4 * (size_t)xo, cudaMemcpyDeviceToHost,
-                                     c->stream)) != cudaSuccess ||
-                (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+            if ((e = ctx_get(c, hops.data(), c->b_ops.p, (size_t)oo)) != cudaSuccess ||
+                (e = ctx_get(c, hxp.data(), c->b_xps.p, sizeof(int64_t) * 4 * (size_t)xo)) != cudaSuccess)
                 return ctx_cuda_fail(c, e, "batch traceback copy");
             out->ops = (char *)std::malloc((size_t)tot_ops + 1);
             out->xpoints = (swb_xpoint *)std::malloc(sizeof(swb_xpoint) * (size_t)(tot_xp + 2 * ntrace + 1));

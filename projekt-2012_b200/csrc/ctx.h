@@ -12,9 +12,13 @@
 namespace swb {
 
 // A device allocation that grows on demand and is reused from call to call.
+// Growth is stream-ordered on the owning context's stream (cudaFreeAsync /
+// cudaMallocAsync): a plain cudaFree would wait for the whole device, stalling
+// every other context on it (the serving loop runs two).
 struct DevBuf {
     void *p = nullptr;
     size_t cap = 0;
+    cudaStream_t st = nullptr;
     cudaError_t ensure(size_t bytes);
     void release();
 };
@@ -40,8 +44,9 @@ struct swb_ctx {
     swb::DevBuf tb[16];  // traceback scratch (ops, crosspoints, state, level-2 stores, recompute and walker buffers)
     // batched path: sequences, encodings, descriptors, per-unit / per-pair records, stores
     swb::DevBuf b_seq, b_rcode, b_ctab, b_pairs, b_units, b_hbuf, b_gbest, b_ubest, b_pbest, b_ctl, b_srows,
-        b_scols, b_walk, b_ops, b_xps, b_state;
+        b_scols, b_walk, b_ops, b_xps, b_state, b_gdir;
     swb::HostBuf h_stage;  // pinned staging for descriptors and results
+    swb::HostBuf h_io;     // pinned staging of ctx_get / ctx_put
     int64_t last_nstrips = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::mutex mu;
@@ -49,6 +54,16 @@ struct swb_ctx {
     int64_t last_nsr = 0, last_n = 0, last_sr_interval = 0;
     int32_t last_launches = 0;  // this library's kernels launched by the last stage 1
     int32_t max_blocks = 0;     // cap on the scoring grids of this context (0 = whole GPU); set by the server
+
+    template <class F>
+    void each_buf(F f) {
+        for (swb::DevBuf *b : {&rows, &cols, &hbuf, &wbest, &best, &errf, &srows, &scols, &work, &flags, &lut,
+                               &rcode, &ctab, &trace, &b_seq, &b_rcode, &b_ctab, &b_pairs, &b_units, &b_hbuf,
+                               &b_gbest, &b_ubest, &b_pbest, &b_ctl, &b_srows, &b_scols, &b_walk, &b_ops, &b_xps,
+                               &b_state, &b_gdir})
+            f(*b);
+        for (swb::DevBuf &b : tb) f(b);
+    }
 };
 
 namespace swb {
@@ -56,5 +71,16 @@ namespace swb {
 // Records a one-line error on the context (and the calling thread) and returns code.
 int ctx_fail(swb_ctx *ctx, int code, const char *fmt, ...);
 int ctx_cuda_fail(swb_ctx *ctx, cudaError_t e, const char *what);
+
+// Host <-> device copies of the context, always through its pinned staging
+// buffer on its stream.  A copy to or from pageable host memory is synchronous in
+// the driver and can hold up other threads' CUDA calls until the copy's stream
+// drains (for a long scoring launch, seconds); with pinned staging a thread
+// waits in cudaStreamSynchronize on its own stream only.
+// ctx_get: waits for the stream, then copies bytes from device src into dst.
+// ctx_put: waits for the stream (the staging buffer may feed an earlier put),
+//          copies src into staging and queues the transfer to device dst.
+cudaError_t ctx_get(swb_ctx *c, void *dst, const void *dev_src, size_t bytes);
+cudaError_t ctx_put(swb_ctx *c, void *dev_dst, const void *src, size_t bytes);
 
 }  // namespace swb

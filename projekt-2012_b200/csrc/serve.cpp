@@ -288,6 +288,14 @@ int swb_server_create(const swb_server_options *opts, const swb_scoring *sc, swb
         delete s;
         return rc;
     }
+    // pinned staging sized up front: growing it later (cudaFreeHost) would stall the device
+    if (s->cs->h_io.ensure(64ULL << 20) != cudaSuccess || s->cl->h_io.ensure(64ULL << 20) != cudaSuccess ||
+        s->cs->h_stage.ensure(16ULL << 20) != cudaSuccess) {
+        swb_ctx_destroy(s->cs);
+        swb_ctx_destroy(s->cl);
+        delete s;
+        return swb::ctx_fail(nullptr, SWB_ENOMEM, "server: pinned staging buffers");
+    }
     s->sms = s->cs->sms;
     if (s->o.reserve_sms >= s->sms) s->o.reserve_sms = std::max(1, s->sms / 8);
     s->per_sm = std::max(1, swb::batch_max_blocks_per_sm(true, true));

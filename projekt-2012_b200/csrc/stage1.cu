@@ -22,7 +22,9 @@
 //     later; a mismatch is re-polled with a bounded wait.
 //   * The grid is persistent and cooperative (every warp resident).  Strip s runs
 //     on block s mod B, warp (s / B) mod 4, so consecutive strips sit on
-//     different SMs and every SM gets the same number of strips (+-1).
+//     different SMs and every SM gets the same number of strips (+-1).  (Claiming
+//     strips from a counter instead lets the block scheduler crowd some SMs, and
+//     the chain of strips then runs at the pace of the most crowded one.)
 //   * Substitution score: with at most four distinct column bytes (DNA) a
 //     per-column table word holds (s - open) for codes 0..3 and one PRMT with a
 //     per-row selector picks the sign-extended score (TAB); otherwise the raw
@@ -174,6 +176,28 @@ int max_blocks_r() {
 }
 
 }  // namespace
+
+// Every kernel of the library asks for the largest shared-memory carveout.  An
+// SM's L1/shared split is fixed while blocks run on it, so a long-running kernel
+// that needs little shared memory would otherwise leave its SMs configured with
+// a small carveout, and another lane's kernel that needs more (the walker) could
+// not be placed beside it until the long kernel ended.
+cudaError_t stage1_configure() {
+    const int c = cudaSharedmemCarveoutMaxShared;
+    const auto A = cudaFuncAttributePreferredSharedMemoryCarveout;
+    cudaError_t e = cudaSuccess;
+    for (cudaError_t x : {cudaFuncSetAttribute((const void *)stage1_kernel<8, false>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<8, true>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<16, false>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<16, true>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<32, false>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<32, true>, A, c),
+                          cudaFuncSetAttribute((const void *)reduce_best_kernel, A, c),
+                          cudaFuncSetAttribute((const void *)encode_kernel, A, c),
+                          cudaFuncSetAttribute((const void *)presence_kernel, A, c)})
+        if (x != cudaSuccess) e = x;
+    return e;
+}
 
 int stage1_max_blocks_per_sm(int R, bool tab) {
     switch (R) {

@@ -96,4 +96,9 @@ cudaError_t stage1_encode(const uint8_t *rows, int64_t m, const uint8_t *cols, i
 
 uint64_t tie_key_host(const TieGeom &g, int64_t r, int64_t c);
 
+// Shared-memory carveout preference of the library's kernels on the current
+// device (stage1.cu, batch.cu, traceback.cu); called when a context is created.
+cudaError_t stage1_configure();
+cudaError_t batch_configure();
+
 }  // namespace swb

@@ -103,9 +103,11 @@ int traceback(cudaStream_t st, int sms, const uint8_t *d_rows, int64_t m, const 
             int32_t corner = 0;
             if (RR0 > 0 && CC0 > 0) {
                 int2 cv;
-                cudaMemcpyAsync(&cv, d_srows + (RR0 / plan.kr - 1) * n + CC0 - 1, sizeof cv, cudaMemcpyDeviceToHost,
-                                st);
-                cudaStreamSynchronize(st);
+                cudaError_t ce = scr.get(scr.owner, &cv, d_srows + (RR0 / plan.kr - 1) * n + CC0 - 1, sizeof cv);
+                if (ce != cudaSuccess) {
+                    err = std::string("level-1 corner: ") + cudaGetErrorString(ce);
+                    return SWB_ECUDA;
+                }
                 corner = cv.x;
             }
             a.top = top;
@@ -158,11 +160,8 @@ int traceback(cudaStream_t st, int sms, const uint8_t *d_rows, int64_t m, const 
         return SWB_ENOMEM;
     }
     cudaError_t e;
-    if ((e = cudaMemcpyAsync(out->ops, d_ops, (size_t)nops, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
-        (nxp > 0 &&
-         (e = cudaMemcpyAsync(hx.data(), d_xps, sizeof(int64_t) * 4 * (size_t)nxp, cudaMemcpyDeviceToHost, st)) !=
-             cudaSuccess) ||
-        (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+    if ((e = scr.get(scr.owner, out->ops, d_ops, (size_t)nops)) != cudaSuccess ||
+        (e = scr.get(scr.owner, hx.data(), d_xps, sizeof(int64_t) * 4 * (size_t)nxp)) != cudaSuccess) {
         err = std::string("traceback copy: ") + cudaGetErrorString(e);
         return SWB_ECUDA;
     }

@@ -12,11 +12,18 @@
 // depend on any tuning parameter of this build.
 //
 // How: stage 1 keeps special rows (H, F) every 512 rows and special columns
-// (H, E) every 256 columns.  The walker kernel is one persistent CTA: for the
-// 512 x 256 block that holds the current cell it recomputes the block up to
-// that cell from the stored boundaries, with one direction byte per cell in
-// shared memory, then warp 0 walks the path (32 cells per ballot along
-// diagonal, row or column runs) until the path leaves the block, and repeats.
+// (H, E) every 256 columns, so every 512 x 256 block of the matrix can be
+// recomputed from its stored boundaries alone, with one direction byte per cell.
+// A block's directions do not depend on the path, so the walker of a single
+// pair (walk_region) recomputes a predicted corridor of whole blocks at once,
+// one CTA per block across the GPU (the staircase of blocks along the diagonal
+// from the current cell, with the blocks above and to the left as margin), and
+// then one warp walks the path through them (32 cells per ballot along
+// diagonal, row or column runs) until it reaches the start or leaves the
+// corridor, where the next round predicts from.  Batches of pairs use one CTA
+// per pair that recomputes the blocks on its path on demand.  Inside a CTA the
+// block recompute is a pipeline of four warps of 128 rows each, handing rows
+// down through shared memory with tagged 64-bit words instead of barriers.
 // Pairs whose stores would not fit the HBM budget keep a coarser grid (level 1);
 // each level-1 cell the path enters is recomputed by the stage-1 kernel on that
 // sub-rectangle, which writes the 512 x 256 stores for it (level 2).
@@ -104,22 +111,9 @@ __device__ void stage_block(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C
     for (int64_t i = threadIdx.x; i < h; i += blockDim.x) s->rb[i] = a.rows[R0 + i];
 }
 
-// Direction byte of block cell (row offset i, column offset j): column-major, so
-// the kRT rows a lane computes for one column are one aligned 32-bit word.
-__device__ __forceinline__ int dix(int64_t i, int64_t j) { return (int)(j * kBR + i); }
-
-// Direction bytes of the block being walked, in shared memory (column-major).
-struct SmemDir {
-    uint8_t *d;
-    __device__ __forceinline__ uint8_t at(int64_t i, int64_t j) const { return d[dix(i, j)]; }
-    __device__ __forceinline__ void put(int t, int64_t j, int64_t /*k*/, uint32_t word) const {
-        *reinterpret_cast<uint32_t *>(d + dix(4 * t, j)) = word;
-    }
-};
-
-// Direction bytes of one precomputed block in global memory, in the recompute's
-// step order so that every warp store is one coalesced 128-byte line: word
-// (warp, k, lane) holds rows 4t .. 4t + 3 (t = 32 warp + lane) of column k - lane.
+// Direction bytes of one block in global memory, in the recompute's step order so
+// that every warp store is one coalesced 128-byte line: word (warp, k, lane)
+// holds rows 4t .. 4t + 3 (t = 32 warp + lane) of column k - lane.
 constexpr int kSteps = kBC + 31;
 constexpr int64_t kBlockWords = (int64_t)(kThreads / 32) * kSteps * 32;
 struct GlobalDir {
@@ -431,7 +425,8 @@ __device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const D &dir, co
 
 // Block after block until the start is reached or the path leaves the region
 // [rr0, .) x [cc0, .); the state is read from and written back to a.st.
-__device__ void walk_body(const WalkArgs &a, uint8_t *dir, Xchg *xc, Stage *sg, int64_t *S) {
+template <class D>
+__device__ void walk_body(const WalkArgs &a, const D &dir, Xchg *xc, Stage *sg, int64_t *S) {
     if (threadIdx.x < kStN) S[threadIdx.x] = a.st[threadIdx.x];
     __syncthreads();
     int guard = 0;
@@ -442,14 +437,14 @@ __device__ void walk_body(const WalkArgs &a, uint8_t *dir, Xchg *xc, Stage *sg, 
         const int64_t C0 = a.cc0 + ((c - a.cc0) / kBC) * kBC;
         stage_block(a, R0, r, C0, c, sg);
         __syncthreads();
-        recompute(a, R0, r, C0, c, SmemDir{dir}, xc, sg, xc->gen + (uint32_t)guard + 1u);
+        recompute(a, R0, r, C0, c, dir, xc, sg, xc->gen + (uint32_t)guard + 1u);
         __syncthreads();
         if (xc->err) {
             if (threadIdx.x == 0) S[kStErr] = 1;
             __syncthreads();
             break;
         }
-        if (threadIdx.x < 32) walk(a, R0, C0, SmemDir{dir}, sg, S);
+        if (threadIdx.x < 32) walk(a, R0, C0, dir, sg, S);
         __syncthreads();
     }
     if (threadIdx.x < kStN) a.st[threadIdx.x] = S[threadIdx.x];
@@ -518,14 +513,15 @@ __global__ void __launch_bounds__(32) corridor_walk_kernel(WalkArgs a, const uin
 }
 
 // Batched pairs: CTA b walks pairs b, b + gridDim.x, ... (each pair's whole
-// matrix is its region).
-__global__ void __launch_bounds__(kThreads) walk_batch_kernel(const WalkArgs *args, int64_t n) {
-    extern __shared__ uint8_t dir[];
+// matrix is its region), recomputing the blocks on its path on demand into its
+// own region of gdir (kBlockWords words per CTA).
+__global__ void __launch_bounds__(kThreads) walk_batch_kernel(const WalkArgs *args, int64_t n, uint32_t *gdir) {
     __shared__ Xchg xc;
     __shared__ Stage sg;
     __shared__ int64_t S[kStN];
     __shared__ WalkArgs sa;
     xchg_init(&xc);
+    const GlobalDir dir{gdir + (int64_t)blockIdx.x * kBlockWords};
     for (int64_t p = blockIdx.x; p < n; p += gridDim.x) {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -538,6 +534,17 @@ __global__ void __launch_bounds__(kThreads) walk_batch_kernel(const WalkArgs *ar
 }
 
 }  // namespace
+
+cudaError_t walker_configure() {
+    const int c = cudaSharedmemCarveoutMaxShared;
+    const auto A = cudaFuncAttributePreferredSharedMemoryCarveout;
+    cudaError_t e = cudaSuccess;
+    for (cudaError_t x : {cudaFuncSetAttribute((const void *)precompute_kernel, A, c),
+                          cudaFuncSetAttribute((const void *)corridor_walk_kernel, A, c),
+                          cudaFuncSetAttribute((const void *)walk_batch_kernel, A, c)})
+        if (x != cudaSuccess) e = x;
+    return e;
+}
 
 int64_t choose_special_interval(const swb_options &opts, int64_t m, int64_t n) {
     (void)opts;
@@ -658,8 +665,7 @@ int walk_region(cudaStream_t st, int sms, const WalkInputs &in, int64_t *host_st
         return SWB_ENOMEM;
     }
     if ((e = cudaMemsetAsync(d_err, 0, sizeof(int32_t), st)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(in.dstate, host_state, sizeof(int64_t) * kStN, cudaMemcpyHostToDevice, st)) !=
-            cudaSuccess) {
+        (e = scr.put(scr.owner, in.dstate, host_state, sizeof(int64_t) * kStN)) != cudaSuccess) {
         err = std::string("walker state: ") + cudaGetErrorString(e);
         return SWB_ECUDA;
     }
@@ -676,10 +682,8 @@ int walk_region(cudaStream_t st, int sms, const WalkInputs &in, int64_t *host_st
             err = "walker buffers: out of device memory";
             return SWB_ENOMEM;
         }
-        if ((e = cudaMemcpyAsync(d_blk, blk.data(), sizeof(int64_t) * blk.size(), cudaMemcpyHostToDevice, st)) !=
-                cudaSuccess ||
-            (e = cudaMemcpyAsync(d_map, map.data(), sizeof(int32_t) * map.size(), cudaMemcpyHostToDevice, st)) !=
-                cudaSuccess) {
+        if ((e = scr.put(scr.owner, d_blk, blk.data(), sizeof(int64_t) * blk.size())) != cudaSuccess ||
+            (e = scr.put(scr.owner, d_map, map.data(), sizeof(int32_t) * map.size())) != cudaSuccess) {
             err = std::string("walker corridor: ") + cudaGetErrorString(e);
             return SWB_ECUDA;
         }
@@ -687,9 +691,7 @@ int walk_region(cudaStream_t st, int sms, const WalkInputs &in, int64_t *host_st
         corridor_walk_kernel<<<1, 32, 0, st>>>(a, gdir, d_map, bi0, bj0, mh, mw, d_err);
         *launches += 2;
         if ((e = cudaGetLastError()) != cudaSuccess ||
-            (e = cudaMemcpyAsync(host_state, in.dstate, sizeof(int64_t) * kStN, cudaMemcpyDeviceToHost, st)) !=
-                cudaSuccess ||
-            (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+            (e = scr.get(scr.owner, host_state, in.dstate, sizeof(int64_t) * kStN)) != cudaSuccess) {
             err = std::string("walker: ") + cudaGetErrorString(e);
             return SWB_ECUDA;
         }
@@ -705,8 +707,13 @@ int walk_region(cudaStream_t st, int sms, const WalkInputs &in, int64_t *host_st
     return SWB_OK;
 }
 
+int64_t walk_batch_ctas(int sms, int64_t n) { return std::max<int64_t>(1, std::min<int64_t>(n, 8LL * std::max(1, sms))); }
+size_t walk_batch_dir_bytes(int sms, int64_t n) {
+    return sizeof(uint32_t) * (size_t)kBlockWords * (size_t)walk_batch_ctas(sms, n);
+}
+
 int walk_batch(cudaStream_t st, int sms, const WalkInputs *in, int64_t n, void *d_args, int64_t *d_states,
-               int64_t *host_states, std::string &err) {
+               void *d_dir, int64_t *host_states, const Scratch &scr, std::string &err) {
     if (n <= 0) return SWB_OK;
     std::vector<WalkArgs> args((size_t)n);
     for (int64_t i = 0; i < n; ++i) {
@@ -714,22 +721,15 @@ int walk_batch(cudaStream_t st, int sms, const WalkInputs *in, int64_t n, void *
         args[(size_t)i].st = d_states + i * kStN;
     }
     cudaError_t e;
-    const size_t smem = (size_t)kBR * kBC;
-    const int64_t grid = std::min<int64_t>(n, (int64_t)std::max(1, sms));
-    if ((e = cudaFuncSetAttribute(walk_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
-            cudaSuccess ||
-        (e = cudaMemcpyAsync(d_args, args.data(), sizeof(WalkArgs) * (size_t)n, cudaMemcpyHostToDevice, st)) !=
-            cudaSuccess ||
-        (e = cudaMemcpyAsync(d_states, host_states, sizeof(int64_t) * kStN * (size_t)n, cudaMemcpyHostToDevice,
-                             st)) != cudaSuccess) {
+    const int64_t grid = walk_batch_ctas(sms, n);
+    if ((e = scr.put(scr.owner, d_args, args.data(), sizeof(WalkArgs) * (size_t)n)) != cudaSuccess ||
+        (e = scr.put(scr.owner, d_states, host_states, sizeof(int64_t) * kStN * (size_t)n)) != cudaSuccess) {
         err = std::string("batched walker set-up: ") + cudaGetErrorString(e);
         return SWB_ECUDA;
     }
-    walk_batch_kernel<<<(unsigned)grid, kThreads, smem, st>>>((const WalkArgs *)d_args, n);
+    walk_batch_kernel<<<(unsigned)grid, kThreads, 0, st>>>((const WalkArgs *)d_args, n, (uint32_t *)d_dir);
     if ((e = cudaGetLastError()) != cudaSuccess ||
-        (e = cudaMemcpyAsync(host_states, d_states, sizeof(int64_t) * kStN * (size_t)n, cudaMemcpyDeviceToHost,
-                             st)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+        (e = scr.get(scr.owner, host_states, d_states, sizeof(int64_t) * kStN * (size_t)n)) != cudaSuccess) {
         err = std::string("batched walker: ") + cudaGetErrorString(e);
         return SWB_ECUDA;
     }

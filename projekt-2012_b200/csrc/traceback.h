@@ -17,6 +17,7 @@ struct Plan {
     int64_t kc = 256;   // special-column spacing (columns), power of two >= 256
 };
 Plan plan_for(const swb_options &opts, int64_t m, int64_t n);
+cudaError_t walker_configure();
 int64_t choose_special_interval(const swb_options &opts, int64_t m, int64_t n);
 
 // Inputs of one walker launch over a region [rr0, rr1) x [cc0, cc1).
@@ -37,11 +38,7 @@ struct WalkInputs {
     int64_t *dstate;              // device copy of the walker state
 };
 
-// Walks n independent pairs (each region is its pair's whole matrix) with one
-// launch; d_args holds n * walk_args_bytes() bytes, d_states n * state_slots()
-// int64 (initial states are copied from host_states, final ones back to it).
-int walk_batch(cudaStream_t st, int sms, const WalkInputs *in, int64_t n, void *d_args, int64_t *d_states,
-               int64_t *host_states, std::string &err);
+
 size_t walk_args_bytes();
 int state_slots();
 int slot_r();
@@ -58,6 +55,9 @@ int block_cols();
 // Device scratch the orchestration needs (owned by the caller's context).
 struct Scratch {
     void *(*ensure)(void *owner, int which, size_t bytes);  // returns device memory or nullptr
+    // copies between host and device through the owner's pinned staging on its stream
+    cudaError_t (*get)(void *owner, void *dst, const void *dev_src, size_t bytes);
+    cudaError_t (*put)(void *owner, void *dev_dst, const void *src, size_t bytes);
     void *owner;
 };
 enum ScratchSlot {
@@ -70,6 +70,14 @@ enum ScratchSlot {
 // whole blocks precomputed in parallel, then walked by one warp.
 int walk_region(cudaStream_t st, int sms, const WalkInputs &in, int64_t *host_state, const Scratch &scr,
                 std::string &err, int32_t *launches);
+
+// Walks n independent pairs (each region is its pair's whole matrix) with one
+// launch; d_args holds n * walk_args_bytes() bytes, d_states n * state_slots()
+// int64 (initial states are copied from host_states, final ones back to it),
+// d_dir walk_batch_dir_bytes(sms, n) bytes of direction scratch.
+int walk_batch(cudaStream_t st, int sms, const WalkInputs *in, int64_t n, void *d_args, int64_t *d_states,
+               void *d_dir, int64_t *host_states, const Scratch &scr, std::string &err);
+size_t walk_batch_dir_bytes(int sms, int64_t n);
 
 // Canonical traceback from the end cell in `out` (score, end_row, end_col set by
 // stage 1), using the stage-1 stores laid out by `plan`.  Fills out->ops,

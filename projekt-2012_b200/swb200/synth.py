@@ -103,3 +103,39 @@ def batched(npairs: int = 100_000, seed_extra: int = 0, sigma: float = 0.75):
         parts.append(target)
         off += L + tlen
     return np.concatenate(parts), refs, (2, -3, -5, -2)
+
+
+def serving_request(rng: np.random.Generator):
+    """One request of the serving mix: 95% short pairs (query uniform 200-5,000 bp,
+    target 1.5x built from the query with 7% substitutions and 1% indels, mean 3,
+    inside random padding) and 5% long pairs (query uniform 100 kbp-2 Mbp, target
+    1.5x with 2.5% substitutions and 0.5% indels, mean 4).  Returns (query, target,
+    is_long)."""
+    long = rng.random() < 0.05
+    if long:
+        L = int(rng.integers(100_000, 2_000_001))
+        sub, indel, mean = 0.025, 0.005, 4.0
+    else:
+        L = int(rng.integers(200, 5_001))
+        sub, indel, mean = 0.07, 0.01, 3.0
+    query = random_dna(rng, L)
+    core = mutate(rng, query, sub, indel, mean)
+    tlen = int(round(1.5 * L))
+    core = core[:tlen]
+    pad = tlen - len(core)
+    left = int(rng.integers(0, pad + 1))
+    target = np.concatenate([random_dna(rng, left), core, random_dna(rng, pad - left)])
+    return query.tobytes(), target.tobytes(), long
+
+
+def serving_stream(duration_s: float, rate: float, seed_extra: int = 0):
+    """Poisson arrivals at `rate` per second for duration_s seconds: list of
+    (arrival time s, query, target, is_long)."""
+    rng = rng_for(4, seed_extra)
+    t, out = 0.0, []
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t >= duration_s:
+            return out
+        q, tg, lg = serving_request(rng)
+        out.append((t, q, tg, lg))
