@@ -64,7 +64,8 @@ def workload(name):
         desc = "plain pair: 2,000 bp vs 400 + mutated 1,200 bp window + 400; scoring 1/-3/-5/-2"
     else:
         a, b, sc = synth.chromosome_pair()
-        desc = "chromosome pair: two ~10 Mbp from an 8 Mbp ancestor (3% sub, 0.5% indel) + 1 Mbp flanks"
+        desc = ("chromosome pair: two ~10 Mbp from an 8 Mbp ancestor (3% sub, 0.5% indel, mean 4) + 1 Mbp "
+                "random flanks on both ends; scoring 1/-3/-5/-2; special rows/columns within a 40 GB budget")
     return a, b, sc, desc
 
 
@@ -355,7 +356,9 @@ def main():
     rows_b, cols_b = (a, b) if len(a) >= len(b) else (b, a)
     cells = m * n
     stream = torch.cuda.current_stream()
-    ctx = swb200.Context(device=local, cuda_stream=stream.cuda_stream)
+    # the chromosome-scale pair keeps its special rows / columns within 40 GB
+    budget = 40_000_000_000 if args.workload == "chromosome" else 0
+    ctx = swb200.Context(device=local, cuda_stream=stream.cuda_stream, hbm_budget_bytes=budget)
     flags = swb200.FLAG_SCORE_ONLY if args.score_only else 0
 
     d_rows = torch.frombuffer(bytearray(rows_b), dtype=torch.uint8).cuda()

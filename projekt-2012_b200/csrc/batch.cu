@@ -29,19 +29,35 @@
 namespace swb {
 namespace {
 
-// Store fields of a pair view: none (score only) or per-pair special rows and
-// columns (store pass for the traceback).
+// Store and boundary fields of a pair view: none (score only), per-pair special
+// rows and columns (store pass for the traceback), or those plus the top / left
+// boundaries of a sub-rectangle (level-1 recompute of the traceback).
 struct NoStores {
     static constexpr int2 *srows = nullptr;
     static constexpr int64_t sr_every = 1;
     static constexpr int2 *scols = nullptr;
     static constexpr int32_t sc_every = 1 << 30;
+    static constexpr const int2 *top = nullptr;
+    static constexpr const int2 *left = nullptr;
+    static constexpr int32_t corner = 0;
 };
 struct WithStores {
     int2 *srows;
     int64_t sr_every;
     int2 *scols;
     int32_t sc_every;
+    static constexpr const int2 *top = nullptr;
+    static constexpr const int2 *left = nullptr;
+    static constexpr int32_t corner = 0;
+};
+struct WithBounds {
+    int2 *srows;
+    int64_t sr_every;
+    int2 *scols;
+    int32_t sc_every;
+    const int2 *top;
+    const int2 *left;
+    int32_t corner;
 };
 
 // The argument view the wavefront core reads for one pair of a batch.
@@ -56,9 +72,6 @@ struct PairView : S {
     int4 *hbuf;
     int32_t *gbest;
     TieGeom tie;
-    static constexpr const int2 *top = nullptr;
-    static constexpr const int2 *left = nullptr;
-    static constexpr int32_t corner = 0;
     static constexpr int64_t r_origin = 0;
     static constexpr int64_t c_origin = 0;
     static constexpr int64_t *trace = nullptr;
@@ -86,7 +99,7 @@ __global__ void __launch_bounds__(kWarps * 32, (std::is_same<S, NoStores>::value
         v.tab_hi = g.tab_hi;
         v.err = g.ctl + 1;
         v.rows = g.seq + d.row_off;
-        v.cols = g.seq + d.col_off;
+        v.cols = g.cseq + d.col_off;
         v.rcode = TAB ? g.rcode + d.row_off : nullptr;
         v.ctab = TAB ? g.ctab + d.col_off : nullptr;
         v.m = d.m;
@@ -99,6 +112,11 @@ __global__ void __launch_bounds__(kWarps * 32, (std::is_same<S, NoStores>::value
             v.sr_every = d.sr_every;
             v.scols = g.scols + d.sc_off;
             v.sc_every = d.sc_every;
+        }
+        if constexpr (std::is_same<S, WithBounds>::value) {
+            v.top = d.top;
+            v.left = d.left;
+            v.corner = (d.top && d.left) ? d.top[-1].x : 0;
         }
         Best b;
         b.ho = g.open + 1;  // only H >= 1 is recorded
@@ -208,22 +226,27 @@ cudaError_t batch_configure() {
                           cudaFuncSetAttribute((const void *)batch_kernel<true, NoStores>, A, c),
                           cudaFuncSetAttribute((const void *)batch_kernel<false, WithStores>, A, c),
                           cudaFuncSetAttribute((const void *)batch_kernel<true, WithStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_kernel<false, WithBounds>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_kernel<true, WithBounds>, A, c),
                           cudaFuncSetAttribute((const void *)batch_reduce_kernel, A, c),
                           cudaFuncSetAttribute((const void *)batch_encode_kernel, A, c)})
         if (x != cudaSuccess) e = x;
     return e;
 }
 
-int batch_max_blocks_per_sm(bool tab, bool stores) {
-    if (stores) return tab ? max_blocks<true, WithStores>() : max_blocks<false, WithStores>();
+int batch_max_blocks_per_sm(bool tab, BatchMode mode) {
+    if (mode == kBatchBounds) return tab ? max_blocks<true, WithBounds>() : max_blocks<false, WithBounds>();
+    if (mode == kBatchStores) return tab ? max_blocks<true, WithStores>() : max_blocks<false, WithStores>();
     return tab ? max_blocks<true, NoStores>() : max_blocks<false, NoStores>();
 }
 
-cudaError_t batch_launch(const BatchArgs &a, bool tab, bool stores, int sms, int max_blocks, int64_t npairs,
+cudaError_t batch_launch(const BatchArgs &a, bool tab, BatchMode mode, int sms, int max_blocks, int64_t npairs,
                          BestRec *pbest, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
     if (a.nunits > 0) {
-        if (stores)
+        if (mode == kBatchBounds)
+            e = tab ? launch<true, WithBounds>(a, sms, max_blocks, st) : launch<false, WithBounds>(a, sms, max_blocks, st);
+        else if (mode == kBatchStores)
             e = tab ? launch<true, WithStores>(a, sms, max_blocks, st) : launch<false, WithStores>(a, sms, max_blocks, st);
         else
             e = tab ? launch<true, NoStores>(a, sms, max_blocks, st) : launch<false, NoStores>(a, sms, max_blocks, st);

@@ -22,13 +22,25 @@ struct BatchPair {
     int32_t ufirst, ucount;    // this launch's units of the pair: [ufirst, ufirst + ucount)
     int32_t pad_;
     TieGeom tie;               // tie rule of the pair (reference launch shape of its lengths)
+    // boundary pass only (a sub-rectangle of a larger matrix): (H, F) of the row
+    // above and (H, E) of the column to the left (nullptr: matrix edge, zero);
+    // the corner H is top[-1] when both exist
+    const int2 *top, *left;
+};
+
+// What a launch computes besides the best cells.
+enum BatchMode : int32_t {
+    kBatchScore = 0,       // scores only
+    kBatchStores = 1,      // special rows / columns of every pair
+    kBatchBounds = 2,      // special rows / columns of sub-rectangles with top / left boundaries
 };
 
 // Uniform arguments of one batched launch.
 struct BatchArgs {
-    const uint8_t *seq;        // sequence bytes (CMP mode)
+    const uint8_t *seq;        // sequence bytes of the rows (CMP mode)
+    const uint8_t *cseq;       // sequence bytes of the columns (CMP mode; usually seq)
     const uint8_t *rcode;      // TAB mode: per-byte code of seq
-    const uint32_t *ctab;      // TAB mode: per-byte table word of seq
+    const uint32_t *ctab;      // TAB mode: per-byte table word of cseq
     int32_t open, ext, gx, mt1, mm1;
     uint32_t tab_hi;
     const BatchPair *pairs;
@@ -50,16 +62,16 @@ constexpr int kBatchStripRows = 32 * kBatchR;
 // first), then merges the strips' best cells of pairs [0, npairs) of a.pairs
 // into pbest[slot] (which holds the pair's best so far, or an invalid record).
 // Every strip a launch runs must have its predecessor strip either earlier in the
-// same launch's unit order or finished by an earlier launch.  `stores` selects
-// the store pass.  max_blocks > 0 caps the grid (the rest of the GPU stays free
+// same launch's unit order or finished by an earlier launch.  `mode` selects
+// what is stored.  max_blocks > 0 caps the grid (the rest of the GPU stays free
 // for other work).
-cudaError_t batch_launch(const BatchArgs &a, bool tab, bool stores, int sms, int max_blocks, int64_t npairs,
+cudaError_t batch_launch(const BatchArgs &a, bool tab, BatchMode mode, int sms, int max_blocks, int64_t npairs,
                          BestRec *pbest, cudaStream_t st);
 // Byte presence flags over a buffer (TAB-mode choice) and the TAB encodings of
 // every byte of seq (rcode[i] = lut[seq[i]], ctab[i] = table word of seq[i]).
 cudaError_t batch_encode(const uint8_t *seq, int64_t bytes, const uint8_t *d_lut, uint8_t *rcode, uint32_t *ctab,
                          int32_t mt1, int32_t mm1, uint32_t *tab_hi, cudaStream_t st);
-int batch_max_blocks_per_sm(bool tab, bool stores);
+int batch_max_blocks_per_sm(bool tab, BatchMode mode);
 
 // Host batch with every pair traced, in one scoring pass that keeps the stores
 // (the serving loop's iteration).  Same contract as swb_batch_align(..., 1.0, ...).

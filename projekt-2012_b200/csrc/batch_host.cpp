@@ -85,6 +85,7 @@ int run_launch(swb_ctx *c, const uint8_t *d_seq, bool tab, const BatchArgs &base
     std::memcpy(hs + bp_bytes, unit_pair.data(), up_bytes);
     BatchArgs a = base;
     a.seq = d_seq;
+    a.cseq = d_seq;
     a.pairs = (const BatchPair *)c->b_pairs.p;
     a.unit_pair = (const int32_t *)c->b_units.p;
     a.nunits = nu;
@@ -102,7 +103,8 @@ int run_launch(swb_ctx *c, const uint8_t *d_seq, bool tab, const BatchArgs &base
         (e = cudaMemsetAsync(a.ctl, 0, 4 * sizeof(int32_t), c->stream)) != cudaSuccess)
         return ctx_cuda_fail(c, e, "batch set-up");
     cudaEventRecord(c->ev0, c->stream);
-    if ((e = batch_launch(a, tab, stores, c->sms, c->max_blocks, np, (BestRec *)c->b_pbest.p, c->stream)) !=
+    if ((e = batch_launch(a, tab, stores ? kBatchStores : kBatchScore, c->sms, c->max_blocks, np,
+                          (BestRec *)c->b_pbest.p, c->stream)) !=
         cudaSuccess)
         return ctx_cuda_fail(c, e, "batch launch");
     cudaEventRecord(c->ev1, c->stream);
@@ -369,7 +371,6 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
                 w.cc1 = d.n;
                 w.rtop = nullptr;
                 w.rleft = nullptr;
-                w.rcorner = 0;
                 w.xp_interval = it.xpoint_interval;
                 w.ops = (char *)c->b_ops.p + oo;
                 w.ops_cap = (int64_t)d.m + d.n + 8;

@@ -41,7 +41,7 @@ struct swb_ctx {
     int sms = 0;
     std::string err;
     swb::DevBuf rows, cols, hbuf, wbest, best, errf, srows, scols, work, flags, lut, rcode, ctab, trace;
-    swb::DevBuf tb[16];  // traceback scratch (ops, crosspoints, state, level-2 stores, recompute and walker buffers)
+    swb::DevBuf tb[24];  // traceback scratch (ops, crosspoints, state, level-2 stores, recompute and walker buffers)
     // batched path: sequences, encodings, descriptors, per-unit / per-pair records, stores
     swb::DevBuf b_seq, b_rcode, b_ctab, b_pairs, b_units, b_hbuf, b_gbest, b_ubest, b_pbest, b_ctl, b_srows,
         b_scols, b_walk, b_ops, b_xps, b_state, b_gdir;

@@ -65,13 +65,15 @@ uint64_t short_footprint(int64_t m, int64_t n) {
 
 // Device bytes a long request holds: the pair path's buffers with its special
 // rows / columns sized to `store_budget`.
-uint64_t long_footprint(int64_t m, int64_t n, uint64_t store_budget) {
+uint64_t long_footprint(int64_t m, int64_t n, uint64_t store_budget, int sms) {
     swb_options o;
     swb_options_default(&o);
     o.hbm_budget_bytes = store_budget;
     const swb::tb::Plan p = swb::tb::plan_for(o, m, n);
     const uint64_t stores = 8ULL * ((uint64_t)(m / p.kr) * n + (uint64_t)(n / p.kc) * m);
-    const uint64_t level2 = p.level1 ? 8ULL * ((uint64_t)(p.kr / 512) * p.kc + (uint64_t)(p.kc / 256) * p.kr) : 0;
+    const uint64_t level2 = p.level1 ? (uint64_t)swb::tb::level1_corridor_cells(p, sms) *
+                                           (uint64_t)swb::tb::level1_cell_store_bytes(p)
+                                     : 0;
     const uint64_t walker = (uint64_t)4 * 148 * 4 * (256 + 31) * 32 * 4;  // precomputed direction blocks
     return 6ULL * (uint64_t)(m + n) + 16ULL * (uint64_t)n + stores + level2 + walker + (uint64_t)(m + n + 8) +
            (64ULL << 20);
@@ -298,7 +300,7 @@ int swb_server_create(const swb_server_options *opts, const swb_scoring *sc, swb
     }
     s->sms = s->cs->sms;
     if (s->o.reserve_sms >= s->sms) s->o.reserve_sms = std::max(1, s->sms / 8);
-    s->per_sm = std::max(1, swb::batch_max_blocks_per_sm(true, true));
+    s->per_sm = std::max(1, swb::batch_max_blocks_per_sm(true, swb::kBatchStores));
     s->ts = std::thread([s] { s->short_lane(); });
     s->tl = std::thread([s] { s->long_lane(); });
     *out = s;
@@ -322,7 +324,7 @@ int swb_server_submit(swb_server *s, const uint8_t *a, int64_t la, const uint8_t
     r->m = std::max(la, lb);
     r->n = std::min(la, lb);
     r->is_long = r->m * r->n > s->o.long_cells;
-    r->foot = r->is_long ? long_footprint(r->m, r->n, s->long_store_budget) : short_footprint(r->m, r->n);
+    r->foot = r->is_long ? long_footprint(r->m, r->n, s->long_store_budget, s->sms) : short_footprint(r->m, r->n);
     r->t_submit = Clock::now();
     if (r->foot > s->o.hbm_budget_bytes) {
         const uint64_t f = r->foot;

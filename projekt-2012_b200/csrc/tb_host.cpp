@@ -6,10 +6,24 @@
 #include <cstring>
 #include <vector>
 
+#include "batch.h"
 #include "traceback.h"
 
 namespace swb {
 namespace tb {
+
+// Level-1 cells recomputed per corridor round: about two waves of strips at 16
+// warps per SM, and at most 8 GiB of their 512 x 256 stores.
+int64_t level1_corridor_cells(const Plan &plan, int sms) {
+    const int64_t strips_per_cell = (plan.kr + block_rows() - 1) / block_rows();
+    const int64_t cell_store = level1_cell_store_bytes(plan);
+    int64_t cap = std::max<int64_t>(3, (2LL * 16 * std::max(1, sms)) / strips_per_cell);
+    return std::min<int64_t>(cap, std::max<int64_t>(3, (int64_t)(8ULL << 30) / std::max<int64_t>(1, cell_store)));
+}
+
+int64_t level1_cell_store_bytes(const Plan &plan) {
+    return 8 * ((plan.kr / block_rows()) * plan.kc + (plan.kc / block_cols()) * plan.kr) + 16 * plan.kc;
+}
 
 int traceback(cudaStream_t st, int sms, const uint8_t *d_rows, int64_t m, const uint8_t *d_cols, int64_t n,
               const swb_scoring *sc, const Plan &plan, const int2 *d_srows, const int2 *d_scols, swb_result *out,
@@ -56,90 +70,158 @@ int traceback(cudaStream_t st, int sms, const uint8_t *d_rows, int64_t m, const 
         w.cc1 = n;
         w.rtop = nullptr;
         w.rleft = nullptr;
-        w.rcorner = 0;
         if ((rc = walk_region(st, sms, w, S.data(), scr, err, launches)) != SWB_OK) return rc;
     } else {
-        // level 1: walk level-1 cell after level-1 cell
-        for (int guard = 0; guard < (1 << 24) && !S[slot_done()]; ++guard) {
+        // level 1: rounds of a predicted corridor of level-1 cells, recomputed at
+        // once by one batched launch that writes each cell's 512 x 256 stores,
+        // then walked cell by cell
+        const int64_t cap = level1_corridor_cells(plan, sms);
+        std::vector<int64_t> cells;  // (RR0, CC0) pairs
+        std::vector<BatchPair> bp;
+        std::vector<int32_t> up;
+        for (int round = 0; round < (1 << 24) && !S[slot_done()]; ++round) {
             const int64_t r = S[slot_r()], c = S[slot_c()];
             if (r < 0 || c < 0) {
                 err = "traceback left the matrix";
                 return SWB_ECUDA;
             }
-            const int64_t RR0 = (r / plan.kr) * plan.kr, CC0 = (c / plan.kc) * plan.kc;
-            const int64_t mm = r - RR0 + 1, nn = c - CC0 + 1;
-            const int64_t nsr2 = mm / kBR, nsc2 = nn / kBC;
-            int2 *s2r = (int2 *)scr.ensure(scr.owner, kScrSrows2, sizeof(int2) * (size_t)std::max<int64_t>(1, nsr2 * nn));
-            int2 *s2c = (int2 *)scr.ensure(scr.owner, kScrScols2, sizeof(int2) * (size_t)std::max<int64_t>(1, nsc2 * mm));
-            Stage1Plan p1 = stage1_plan(mm, nn, sms, 16, false);
-            const int64_t W = (int64_t)p1.blocks * p1.warps_per_block;
-            int4 *hb = (int4 *)scr.ensure(scr.owner, kScrHbuf, sizeof(int4) * (size_t)nn);
-            BestRec *wb = (BestRec *)scr.ensure(scr.owner, kScrWbest, sizeof(BestRec) * (size_t)W);
-            BestRec *bb = (BestRec *)scr.ensure(scr.owner, kScrBest, sizeof(BestRec));
-            int32_t *ee = (int32_t *)scr.ensure(scr.owner, kScrErr, 4 * sizeof(int32_t));
-            if (!s2r || !s2c || !hb || !wb || !bb || !ee) {
+            // corridor: the staircase of level-1 cells along the diagonal from (r, c),
+            // with the cell above and the cell to the left of each as margin
+            cells.clear();
+            auto add = [&](int64_t bi, int64_t bj) {
+                if (bi < 0 || bj < 0 || (int64_t)cells.size() / 2 >= cap) return;
+                for (size_t q = cells.size() >= 16 ? cells.size() - 16 : 0; q < cells.size(); q += 2)
+                    if (cells[q] == bi * plan.kr && cells[q + 1] == bj * plan.kc) return;
+                cells.push_back(bi * plan.kr);
+                cells.push_back(bj * plan.kc);
+            };
+            {
+                int64_t rr = r, ccc = c, bi = r / plan.kr, bj = c / plan.kc;
+                add(bi, bj);
+                add(bi - 1, bj);
+                add(bi, bj - 1);
+                while ((int64_t)cells.size() / 2 < cap) {
+                    const int64_t d = std::min(rr - bi * plan.kr + 1, ccc - bj * plan.kc + 1);
+                    rr -= d;
+                    ccc -= d;
+                    if (rr < 0 || ccc < 0) break;
+                    bi = rr / plan.kr;
+                    bj = ccc / plan.kc;
+                    add(bi, bj);
+                    add(bi - 1, bj);
+                    add(bi, bj - 1);
+                }
+            }
+            const int64_t ncell = (int64_t)cells.size() / 2;
+            // one batched launch: every cell is a sub-rectangle with its boundaries
+            bp.assign((size_t)ncell, BatchPair{});
+            up.clear();
+            int64_t hb = 0, srn = 0, scn = 0;
+            for (int64_t q = 0; q < ncell; ++q) {
+                const int64_t RR0 = cells[2 * q], CC0 = cells[2 * q + 1];
+                const int64_t mm = std::min(plan.kr, m - RR0), nn = std::min(plan.kc, n - CC0);
+                BatchPair &d = bp[(size_t)q];
+                d.row_off = RR0;
+                d.col_off = CC0;
+                d.m = (int32_t)mm;
+                d.n = (int32_t)nn;
+                d.nstrips = (int32_t)((mm + kBatchStripRows - 1) / kBatchStripRows);
+                d.unit0 = d.ufirst = (int32_t)up.size();
+                d.ucount = d.nstrips;
+                d.slot = (int32_t)q;
+                d.hbuf_off = hb;
+                hb += nn;
+                d.sr_every = 1;
+                d.sc_every = kBC;
+                d.sr_off = srn;
+                d.sc_off = scn;
+                srn += (mm / kBR) * nn;
+                scn += (nn / kBC) * mm;
+                d.tie.mode = kTieRowMajor;
+                d.tie.G = d.tie.T = 1;
+                d.tie.C = 1;
+                d.top = RR0 > 0 ? d_srows + (RR0 / plan.kr - 1) * n + CC0 : nullptr;
+                d.left = CC0 > 0 ? d_scols + (CC0 / plan.kc - 1) * m + RR0 : nullptr;
+                for (int32_t u = 0; u < d.nstrips; ++u) up.push_back((int32_t)q);
+            }
+            BatchPair *dp = (BatchPair *)scr.ensure(scr.owner, kScrL1Pairs, sizeof(BatchPair) * bp.size());
+            int32_t *du = (int32_t *)scr.ensure(scr.owner, kScrL1Units, sizeof(int32_t) * up.size());
+            int4 *dh = (int4 *)scr.ensure(scr.owner, kScrL1Hbuf, sizeof(int4) * (size_t)std::max<int64_t>(1, hb));
+            int32_t *dg = (int32_t *)scr.ensure(scr.owner, kScrL1Gbest, sizeof(int32_t) * (size_t)ncell);
+            BestRec *dub = (BestRec *)scr.ensure(scr.owner, kScrL1Ubest, sizeof(BestRec) * up.size());
+            BestRec *dpb = (BestRec *)scr.ensure(scr.owner, kScrL1Pbest, sizeof(BestRec) * (size_t)ncell);
+            int32_t *dc = (int32_t *)scr.ensure(scr.owner, kScrL1Ctl, 4 * sizeof(int32_t));
+            int2 *s2r = (int2 *)scr.ensure(scr.owner, kScrSrows2, sizeof(int2) * (size_t)std::max<int64_t>(1, srn));
+            int2 *s2c = (int2 *)scr.ensure(scr.owner, kScrScols2, sizeof(int2) * (size_t)std::max<int64_t>(1, scn));
+            if (!dp || !du || !dh || !dg || !dub || !dpb || !dc || !s2r || !s2c) {
                 err = "level-1 recompute buffers: out of device memory";
                 return SWB_ENOMEM;
             }
-            Stage1Args a{};
-            a.rows = d_rows + RR0;
-            a.cols = d_cols + CC0;
-            a.m = mm;
-            a.n = nn;
-            a.open = sc->gap_open;
-            a.ext = sc->gap_extend;
-            a.gx = std::max(sc->gap_open, sc->gap_extend);
-            a.mt1 = sc->match - sc->gap_open;
-            a.mm1 = sc->mismatch - sc->gap_open;
-            a.hbuf = hb;
-            a.srows = nsr2 > 0 ? s2r : nullptr;
-            a.sr_every = 1;
-            a.nsr = nsr2;
-            a.scols = nsc2 > 0 ? s2c : nullptr;
-            a.sc_every = kBC;
-            a.nsc = nsc2;
-            const int2 *top = RR0 > 0 ? d_srows + (RR0 / plan.kr - 1) * n + CC0 : nullptr;
-            const int2 *left = CC0 > 0 ? d_scols + (CC0 / plan.kc - 1) * m + RR0 : nullptr;
-            int32_t corner = 0;
-            if (RR0 > 0 && CC0 > 0) {
-                int2 cv;
-                cudaError_t ce = scr.get(scr.owner, &cv, d_srows + (RR0 / plan.kr - 1) * n + CC0 - 1, sizeof cv);
-                if (ce != cudaSuccess) {
-                    err = std::string("level-1 corner: ") + cudaGetErrorString(ce);
-                    return SWB_ECUDA;
-                }
-                corner = cv.x;
-            }
-            a.top = top;
-            a.left = left;
-            a.corner = corner;
-            a.r_origin = RR0;
-            a.c_origin = CC0;
-            a.nstrips = p1.nstrips;
-            a.wbest = wb;
-            a.best = bb;
-            a.err = ee;
-            a.gbest = a.err + 2;
-            a.trace = nullptr;
-            a.tie.mode = kTieRowMajor;
+            BatchArgs ba{};
+            ba.seq = d_rows;
+            ba.cseq = d_cols;
+            ba.open = sc->gap_open;
+            ba.ext = sc->gap_extend;
+            ba.gx = std::max(sc->gap_open, sc->gap_extend);
+            ba.mt1 = sc->match - sc->gap_open;
+            ba.mm1 = sc->mismatch - sc->gap_open;
+            ba.pairs = dp;
+            ba.unit_pair = du;
+            ba.nunits = (int64_t)up.size();
+            ba.hbuf = dh;
+            ba.gbest = dg;
+            ba.ubest = dub;
+            ba.ctl = dc;
+            ba.srows = s2r;
+            ba.scols = s2c;
             cudaError_t e;
-            if ((e = cudaMemsetAsync(hb, 0xFF, sizeof(int4) * (size_t)nn, st)) != cudaSuccess ||
-                (e = cudaMemsetAsync(ee, 0, 4 * sizeof(int32_t), st)) != cudaSuccess ||
-                (e = stage1_launch(a, p1, st)) != cudaSuccess) {
+            if ((e = scr.put(scr.owner, dp, bp.data(), sizeof(BatchPair) * bp.size())) != cudaSuccess ||
+                (e = scr.put(scr.owner, du, up.data(), sizeof(int32_t) * up.size())) != cudaSuccess ||
+                (e = cudaMemsetAsync(dh, 0xFF, sizeof(int4) * (size_t)std::max<int64_t>(1, hb), st)) != cudaSuccess ||
+                (e = cudaMemsetAsync(dg, 0, sizeof(int32_t) * (size_t)ncell, st)) != cudaSuccess ||
+                (e = cudaMemsetAsync(dpb, 0, sizeof(BestRec) * (size_t)ncell, st)) != cudaSuccess ||
+                (e = cudaMemsetAsync(dc, 0, 4 * sizeof(int32_t), st)) != cudaSuccess ||
+                (e = batch_launch(ba, false, kBatchBounds, sms, 0, ncell, dpb, st)) != cudaSuccess) {
                 err = std::string("level-1 recompute: ") + cudaGetErrorString(e);
                 return SWB_ECUDA;
             }
             *launches += 2;
-            w.srows = s2r;
-            w.scols = s2c;
-            w.rr0 = RR0;
-            w.cc0 = CC0;
-            w.rr1 = RR0 + mm;
-            w.cc1 = CC0 + nn;
-            w.rtop = top;
-            w.rleft = left;
-            w.rcorner = corner;
-            if ((rc = walk_region(st, sms, w, S.data(), scr, err, launches)) != SWB_OK) return rc;
+            int32_t ctl[4];
+            if ((e = scr.get(scr.owner, ctl, dc, sizeof ctl)) != cudaSuccess) {
+                err = std::string("level-1 recompute: ") + cudaGetErrorString(e);
+                return SWB_ECUDA;
+            }
+            if (ctl[1] != 0) {
+                err = "level-1 recompute: a bounded wait between strips ran out";
+                return SWB_ETIMEOUT;
+            }
+            // walk cell after cell while the path stays in the corridor
+            for (;;) {
+                const int64_t rr = S[slot_r()], ccc = S[slot_c()];
+                if (S[slot_done()] || rr < 0 || ccc < 0) break;
+                const int64_t RR0 = (rr / plan.kr) * plan.kr, CC0 = (ccc / plan.kc) * plan.kc;
+                int64_t q = -1;
+                for (int64_t t = 0; t < ncell; ++t)
+                    if (cells[2 * t] == RR0 && cells[2 * t + 1] == CC0) {
+                        q = t;
+                        break;
+                    }
+                if (q < 0) break;  // left the corridor: next round
+                const BatchPair &d = bp[(size_t)q];
+                w.srows = s2r + d.sr_off;
+                w.scols = s2c + d.sc_off;
+                w.rr0 = RR0;
+                w.cc0 = CC0;
+                w.rr1 = RR0 + d.m;
+                w.cc1 = CC0 + d.n;
+                w.rtop = d.top;
+                w.rleft = d.left;
+                if ((rc = walk_region(st, sms, w, S.data(), scr, err, launches)) != SWB_OK) return rc;
+                if (S[slot_r()] == rr && S[slot_c()] == ccc && !S[slot_done()]) {
+                    err = "traceback made no progress in a level-1 cell";
+                    return SWB_ECUDA;
+                }
+            }
         }
         if (!S[slot_done()]) {
             err = "traceback did not finish";

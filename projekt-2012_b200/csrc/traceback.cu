@@ -61,7 +61,6 @@ struct WalkArgs {
     int64_t rr1, cc1;              // region end (exclusive) for store indexing
     const int2 *rtop;              // (H, F) of row rr0 - 1 over region cols (nullptr: zero)
     const int2 *rleft;             // (H, E) of col cc0 - 1 over region rows (nullptr: zero)
-    int32_t rcorner;               // H at (rr0 - 1, cc0 - 1)
     int32_t xp_interval;           // reference special-row spacing (4T)
     char *ops;                     // reversed op stream (end -> start)
     int64_t ops_cap;
@@ -78,7 +77,7 @@ __device__ __forceinline__ int2 top_hf(const WalkArgs &a, int64_t R0, int64_t c)
     // (H, F) of row R0 - 1 at column c (c >= cc0 - 1 handled by callers)
     if (R0 == 0) return make_int2(0, 0);
     if (R0 == a.rr0) {
-        if (c < a.cc0) return make_int2(a.rcorner, 0);
+        if (c < a.cc0) return make_int2((a.rtop && a.rleft) ? a.rtop[-1].x : 0, 0);  // the corner
         return a.rtop ? a.rtop[c - a.cc0] : make_int2(0, 0);
     }
     const int64_t q = (R0 - a.rr0) / kBR - 1;
@@ -592,7 +591,6 @@ static WalkArgs to_args(const WalkInputs &in) {
     a.cc1 = in.cc1;
     a.rtop = in.rtop;
     a.rleft = in.rleft;
-    a.rcorner = in.rcorner;
     a.xp_interval = in.xp_interval;
     a.ops = in.ops;
     a.ops_cap = in.ops_cap;

@@ -17,6 +17,10 @@ struct Plan {
     int64_t kc = 256;   // special-column spacing (columns), power of two >= 256
 };
 Plan plan_for(const swb_options &opts, int64_t m, int64_t n);
+// Level-1 traceback: cells recomputed per corridor round, and device bytes per
+// cell (its 512 x 256 stores and row hand-off buffer).
+int64_t level1_corridor_cells(const Plan &plan, int sms);
+int64_t level1_cell_store_bytes(const Plan &plan);
 cudaError_t walker_configure();
 int64_t choose_special_interval(const swb_options &opts, int64_t m, int64_t n);
 
@@ -28,8 +32,8 @@ struct WalkInputs {
     int32_t score;
     const int2 *srows, *scols;    // the region's 512 x 256 stores
     int64_t rr0, cc0, rr1, cc1;
-    const int2 *rtop, *rleft;     // region boundary (nullptr = matrix edge)
-    int32_t rcorner;
+    const int2 *rtop, *rleft;     // region boundary (nullptr = matrix edge); the corner H is
+                                  // rtop[-1] when both exist
     int32_t xp_interval;
     char *ops;
     int64_t ops_cap;
@@ -62,7 +66,8 @@ struct Scratch {
 };
 enum ScratchSlot {
     kScrOps = 0, kScrXps, kScrState, kScrSrows2, kScrScols2, kScrHbuf, kScrWbest, kScrBest, kScrErr,
-    kScrGdir, kScrBlk, kScrMap, kScrWalkErr, kScrSlots
+    kScrGdir, kScrBlk, kScrMap, kScrWalkErr,
+    kScrL1Pairs, kScrL1Units, kScrL1Hbuf, kScrL1Gbest, kScrL1Ubest, kScrL1Pbest, kScrL1Ctl, kScrSlots
 };
 
 // Walks the path from host_state's cell through the region of `in` (until the

@@ -85,6 +85,39 @@ def test_level1_mode_matches_oracle():
             assert r.kernel_launches > 4
 
 
+def _shifted_pair(rng, m, cut_lo, cut_len, ins_len, sub=0.03):
+    """B = A with a deletion of cut_len bases at cut_lo and an insertion of ins_len
+    random bases further on: the alignment runs off the main diagonal, so the
+    walker's predicted corridors miss and it has to predict again."""
+    a = bytes(rng.choice(b"ACGT") for _ in range(m))
+    core = bytearray(a[:cut_lo] + a[cut_lo + cut_len:])
+    for i in range(len(core)):
+        if rng.random() < sub:
+            core[i] = rng.choice(b"ACGT")
+    at = len(core) * 3 // 4
+    core[at:at] = bytes(rng.choice(b"ACGT") for _ in range(ins_len))
+    return a, bytes(core)
+
+
+def test_path_far_off_the_diagonal(gpu_ctx):
+    rng = random.Random(707)
+    for m, cut_lo, cut_len, ins_len in [(12000, 3000, 2500, 1800), (9000, 500, 4000, 300)]:
+        a, b = _shifted_pair(rng, m, cut_lo, cut_len, ins_len)
+        _check(gpu_ctx, a, b, (1, -3, -5, -2))
+        _check(gpu_ctx, a, b, (2, -3, -5, -2))
+
+
+def test_level1_corridor_off_the_diagonal():
+    """Level-1 cells (coarse grid forced by a small budget) along a path with
+    long gaps: several corridor rounds of level-1 recomputes."""
+    rng = random.Random(808)
+    with swb200.Context(device=0, hbm_budget_bytes=2 << 20) as ctx:
+        a, b = _shifted_pair(rng, 16000, 4000, 3000, 1500)
+        _check(ctx, a, b, (1, -3, -5, -2))
+        a, b = _similar_pair(rng, 14000, 0.9)
+        _check(ctx, a, b, (2, -3, -5, -2))
+
+
 def test_reference_fixtures(gpu_ctx):
     for fa, fb, sc_t in [("1/A00142.fna.gz", "1/A00145.fna.gz", (5, -5, -5, -5)),
                          ("2/NC_005046.fna.gz", "2/NC_012557.fna.gz", (5, -5, -5, -5)),
