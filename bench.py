@@ -34,7 +34,7 @@ def parse_args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["long", "long200k", "long1mx250k", "small", "chromosome"],
+    p.add_argument("--workload", choices=["long", "long200k", "long1mx250k", "tall10mx100k", "small", "chromosome"],
                    default="long")
     p.add_argument("--score-only", action="store_true", help="stage 1 only (diagnostics)")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -59,6 +59,10 @@ def workload(name):
         b = b[:250_000]
         desc = ("the 1 Mbp long pair's rows against the first 250 kbp of its columns (same strip "
                 "count and occupancy as the full pair, a quarter of the steps), for profiling")
+    elif name == "tall10mx100k":
+        a, b, sc = synth.tall_pair()
+        desc = ("10 Mbp iid rows against a mutated 100 kbp window of them (same strip count and occupancy "
+                "as the chromosome-scale pair, 1% of its cells), for profiling")
     elif name == "small":
         a, b, sc = synth.plain_small()
         desc = "plain pair: 2,000 bp vs 400 + mutated 1,200 bp window + 400; scoring 1/-3/-5/-2"

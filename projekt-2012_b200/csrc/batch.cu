@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(kWarps * 32, (std::is_same<S, NoStores>::value
         b.row = 0;
         b.col = 0;
         int32_t bho = b.ho;
-        if (!run_strip<kBatchR, TAB>(v, ring, lane, u - d.unit0, &b, bho)) {
+        if (!run_strip<kBatchR, TAB, !std::is_same<S, NoStores>::value>(v, ring, lane, u - d.unit0, &b, bho)) {
             if (lane == 0) {
                 atomicCAS(&g.ctl[1], kErrNone, kErrTimeout);
                 atomicExch(&g.ctl[2], 1);

@@ -50,7 +50,7 @@ namespace swb {
 
 namespace {
 
-template <int R, bool TAB>
+template <int R, bool TAB, bool STORES>
 __global__ void __launch_bounds__(kWarps * 32, (R <= 16 ? 4 : 2)) stage1_kernel(Stage1Args a) {
     __shared__ int4 ring_all[kWarps][kRing];
     const int lane = threadIdx.x & 31;
@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(kWarps * 32, (R <= 16 ? 4 : 2)) stage1_kernel(
             asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
             a.trace[3 * s + 2] = (int64_t)smid;
         }
-        if (!run_strip<R, TAB>(a, ring, lane, (int32_t)s, &b, bho)) failed = true;
+        if (!run_strip<R, TAB, STORES>(a, ring, lane, (int32_t)s, &b, bho)) failed = true;
         if (a.trace && lane == 0) {
             unsigned long long t;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -160,8 +160,9 @@ __global__ void presence_kernel(const uint8_t *seq, int64_t n, uint32_t *flags) 
 template <int R, bool TAB>
 cudaError_t launch_r(Stage1Args &a, const Stage1Plan &p, cudaStream_t st) {
     void *args[] = {&a};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void *)stage1_kernel<R, TAB>, dim3(p.blocks),
-                                                dim3(kWarps * 32), args, 0, st);
+    const void *fn = (a.srows || a.scols) ? (const void *)stage1_kernel<R, TAB, true>
+                                          : (const void *)stage1_kernel<R, TAB, false>;
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(p.blocks), dim3(kWarps * 32), args, 0, st);
     if (e != cudaSuccess) return e;
     reduce_best_kernel<<<1, 256, 0, st>>>(a.wbest, (int64_t)p.blocks * kWarps, a.best);
     return cudaGetLastError();
@@ -169,10 +170,12 @@ cudaError_t launch_r(Stage1Args &a, const Stage1Plan &p, cudaStream_t st) {
 
 template <int R, bool TAB>
 int max_blocks_r() {
-    int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, stage1_kernel<R, TAB>, kWarps * 32, 0) != cudaSuccess)
+    int nb = 0, ns = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, stage1_kernel<R, TAB, false>, kWarps * 32, 0) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ns, stage1_kernel<R, TAB, true>, kWarps * 32, 0) != cudaSuccess)
         return 0;
-    return nb;
+    return nb < ns ? nb : ns;
 }
 
 }  // namespace
@@ -186,12 +189,18 @@ cudaError_t stage1_configure() {
     const int c = cudaSharedmemCarveoutMaxShared;
     const auto A = cudaFuncAttributePreferredSharedMemoryCarveout;
     cudaError_t e = cudaSuccess;
-    for (cudaError_t x : {cudaFuncSetAttribute((const void *)stage1_kernel<8, false>, A, c),
-                          cudaFuncSetAttribute((const void *)stage1_kernel<8, true>, A, c),
-                          cudaFuncSetAttribute((const void *)stage1_kernel<16, false>, A, c),
-                          cudaFuncSetAttribute((const void *)stage1_kernel<16, true>, A, c),
-                          cudaFuncSetAttribute((const void *)stage1_kernel<32, false>, A, c),
-                          cudaFuncSetAttribute((const void *)stage1_kernel<32, true>, A, c),
+    for (cudaError_t x : {cudaFuncSetAttribute((const void *)stage1_kernel<8, false, false>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<8, true, false>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<16, false, false>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<16, true, false>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<32, false, false>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<32, true, false>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<8, false, true>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<8, true, true>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<16, false, true>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<16, true, true>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<32, false, true>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<32, true, true>, A, c),
                           cudaFuncSetAttribute((const void *)reduce_best_kernel, A, c),
                           cudaFuncSetAttribute((const void *)encode_kernel, A, c),
                           cudaFuncSetAttribute((const void *)presence_kernel, A, c)})

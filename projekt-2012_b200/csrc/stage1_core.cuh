@@ -122,7 +122,8 @@ struct StripCtx {
 };
 
 // One anti-diagonal step.  PRED: some lanes of the warp are outside [0, n).
-// SC: this step may be a special-column step of some lane.
+// SC: this step may be a special-column step of some lane.  SR: the strip's
+// bottom row may be a special row (when false the store is compiled out).
 //
 // Phase 1 computes, for every row of the lane, E and t = max(H_diag + s, E, 0)
 // (independent of the vertical chain); phase 2 runs the F chain and writes HO.
@@ -130,7 +131,7 @@ struct StripCtx {
 // copies are needed.  The column maximum is taken over t: a cell whose H comes
 // from F is strictly below the cell above it, so it can never hold the best
 // score, and a best cell always has H = t.
-template <int R, bool TAB, bool PRED, bool SC, class A>
+template <int R, bool TAB, bool PRED, bool SC, bool SR, class A>
 __device__ __forceinline__ void step(Lane<R> &L, const A &a, Best *b, const int4 *ring, int lane,
                                      const StripCtx &sc, int32_t k) {
     const int32_t j = k - lane;
@@ -184,7 +185,7 @@ __device__ __forceinline__ void step(Lane<R> &L, const A &a, Best *b, const int4
     const bool last = (lane == 31);
     if (last && act) {
         if (sc.below) st_ll(a.hbuf + j, L.HO[R - 1], f, sc.strip);
-        if (sc.sr) a.srows[sc.sr_off + j] = make_int2(L.HO[R - 1] - a.open, flast);
+        if (SR && sc.sr) a.srows[sc.sr_off + j] = make_int2(L.HO[R - 1] - a.open, flast);
     }
     const int32_t oHO = last ? rv.x : L.HO[R - 1];
     const int32_t oF = last ? rv.y : f;
@@ -283,7 +284,10 @@ __device__ __forceinline__ bool refill(const A &a, int4 *ring, int lane, int32_t
     return all_ok;
 }
 
-template <int R, bool TAB, class A>
+// STORES: the launch may write special rows or columns (a.srows or a.scols set).
+// Kernels are instantiated per mode so that each holds only the step bodies it
+// runs (the step loop's speed depends on what else is compiled into it).
+template <int R, bool TAB, bool STORES, class A>
 __device__ bool run_strip(const A &a, int4 *ring, int lane, int32_t s, Best *b, int32_t &bho) {
     Lane<R> L;
     StripCtx sc;
@@ -359,25 +363,33 @@ __device__ bool run_strip(const A &a, int4 *ring, int lane, int32_t s, Best *b, 
     int32_t k = 0;
     for (; k < kA; ++k) {
         if (k > 0 && (k % kCH) == 0 && !refill<TAB>(a, ring, lane, s, n, k, pre, L.thr, L.bho, gpre)) return false;
-        if (a.scols) step<R, TAB, true, true>(L, a, b, ring, lane, sc, k);
-        else step<R, TAB, true, false>(L, a, b, ring, lane, sc, k);
+        if constexpr (!STORES) step<R, TAB, true, false, false>(L, a, b, ring, lane, sc, k);
+        else if (a.scols) step<R, TAB, true, true, true>(L, a, b, ring, lane, sc, k);
+        else step<R, TAB, true, false, true>(L, a, b, ring, lane, sc, k);
     }
     while (k < kB) {
         if (!refill<TAB>(a, ring, lane, s, n, k, pre, L.thr, L.bho, gpre)) return false;
         // lane l stores special column j = q*sc_every - 1 at step j + l: a chunk of
         // steps [k, k+kCH) needs the check when some (t + 1) mod sc_every < 32
         const bool sc_window = a.scols != nullptr && ((k + kCH) & (a.sc_every - 1)) < 32 + kCH;
-        if (sc_window) {
-            for (int u = 0; u < kCH; ++u) step<R, TAB, false, true>(L, a, b, ring, lane, sc, k + u);
+        // Score-only launches run an unrolled chunk; launches with stores keep
+        // their chunks rolled (measured on the 1 Mbp pair: unrolling the scoring
+        // chunk saves about 8%, unrolled chunks with stores cost 20-130%).
+        if constexpr (!STORES) {
+#pragma unroll
+            for (int u = 0; u < kCH; ++u) step<R, TAB, false, false, false>(L, a, b, ring, lane, sc, k + u);
+        } else if (sc_window) {
+            for (int u = 0; u < kCH; ++u) step<R, TAB, false, true, true>(L, a, b, ring, lane, sc, k + u);
         } else {
-            for (int u = 0; u < kCH; ++u) step<R, TAB, false, false>(L, a, b, ring, lane, sc, k + u);
+            for (int u = 0; u < kCH; ++u) step<R, TAB, false, false, true>(L, a, b, ring, lane, sc, k + u);
         }
         k += kCH;
     }
     for (; k < kEnd; ++k) {
         if ((k % kCH) == 0 && !refill<TAB>(a, ring, lane, s, n, k, pre, L.thr, L.bho, gpre)) return false;
-        if (a.scols) step<R, TAB, true, true>(L, a, b, ring, lane, sc, k);
-        else step<R, TAB, true, false>(L, a, b, ring, lane, sc, k);
+        if constexpr (!STORES) step<R, TAB, true, false, false>(L, a, b, ring, lane, sc, k);
+        else if (a.scols) step<R, TAB, true, true, true>(L, a, b, ring, lane, sc, k);
+        else step<R, TAB, true, false, true>(L, a, b, ring, lane, sc, k);
     }
     bho = L.bho;
     return true;

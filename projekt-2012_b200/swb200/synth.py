@@ -139,3 +139,13 @@ def serving_stream(duration_s: float, rate: float, seed_extra: int = 0):
             return out
         q, tg, lg = serving_request(rng)
         out.append((t, q, tg, lg))
+
+
+def tall_pair(rows: int = 10_000_000, cols: int = 100_000, seed_extra: int = 0):
+    """Profiling shape: `rows` iid bases against a mutated `cols`-long window of
+    them (5% sub, 1% indel, mean 4); scoring 1/-3/-5/-2."""
+    rng = rng_for(2, 1000 + seed_extra)
+    a = random_dna(rng, rows)
+    lo = rows // 2
+    b = mutate(rng, a[lo:lo + cols], 0.05, 0.01, 4.0)
+    return a.tobytes(), b.tobytes(), (1, -3, -5, -2)
