@@ -255,9 +255,6 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
                const swb_scoring *sc, uint32_t flags, int64_t sr_interval_rows, int64_t sc_interval,
                swb::BestRec *best_out, float *ms_out, int64_t *nsr_out) {
     using namespace swb;
-    int R = 16;
-    if (const char *rv = std::getenv("SWB_STAGE1_R")) R = std::atoi(rv);  // tuning override: 8, 16 or 32
-    if (sr_interval_rows > 0 && (R > 16 || sr_interval_rows % (32 * R) != 0)) R = 16;  // strips must tile the rows
     cudaError_t e;
     // TAB mode when the column sequence has at most four distinct bytes and the
     // shifted scores fit a signed byte
@@ -276,11 +273,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
         for (int i = 0; i < 256; ++i) lut[i] = present[i] ? (uint8_t)(K++) : 7;
         tab = K <= 4;
     }
-    Stage1Plan plan = stage1_plan(m, n, c->sms, R, tab);
-    if (c->max_blocks > 0 && plan.blocks > c->max_blocks) plan.blocks = c->max_blocks;
-    const int64_t W = (int64_t)plan.blocks * plan.warps_per_block;
     if ((e = c->hbuf.ensure(sizeof(int4) * (size_t)std::max<int64_t>(n, 1))) != cudaSuccess ||
-        (e = c->wbest.ensure(sizeof(BestRec) * (size_t)W)) != cudaSuccess ||
         (e = c->best.ensure(sizeof(BestRec))) != cudaSuccess ||
         (e = c->errf.ensure(4 * sizeof(int32_t))) != cudaSuccess)
         return ctx_cuda_fail(c, e, "stage 1 buffers");
@@ -307,11 +300,31 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
         a.ctab = (const uint32_t *)c->ctab.p;
     }
     a.hbuf = (int4 *)c->hbuf.p;
-    a.nstrips = plan.nstrips;
-    a.wbest = (BestRec *)c->wbest.p;
     a.best = (BestRec *)c->best.p;
     a.err = (int32_t *)c->errf.p;
     a.gbest = a.err + 2;
+    int32_t G = 0, T = 0;
+    int64_t P1 = 0, P2 = 0;
+    const bool refok = reference_geometry(m, n, &G, &T, &P1, &P2);
+    a.tie.mode = ((flags & SWB_FLAG_TIE_ROWMAJOR) || !refok) ? kTieRowMajor : kTieReference;
+    a.tie.G = G;
+    a.tie.T = T;
+    a.tie.C = refok ? P2 / G : 1;
+
+    // rows per lane: an override, else the autotuner (strips must tile the
+    // special-row spacing when special rows are kept)
+    const bool stores = sr_interval_rows > 0 || sc_interval > 0;
+    int R = 16;
+    if (const char *rv = std::getenv("SWB_STAGE1_R")) R = std::atoi(rv);  // override: 8, 16 or 32
+    else R = autotune_rows_per_lane(c, a, tab, stores, 16);
+    if (sr_interval_rows > 0 && (R > 16 || sr_interval_rows % (32 * R) != 0)) R = 16;
+    Stage1Plan plan = stage1_plan(m, n, c->sms, R, tab);
+    if (c->max_blocks > 0 && plan.blocks > c->max_blocks) plan.blocks = c->max_blocks;
+    const int64_t W = (int64_t)plan.blocks * plan.warps_per_block;
+    if ((e = c->wbest.ensure(sizeof(BestRec) * (size_t)W)) != cudaSuccess)
+        return ctx_cuda_fail(c, e, "stage 1 buffers");
+    a.nstrips = plan.nstrips;
+    a.wbest = (BestRec *)c->wbest.p;
     a.srows = nullptr;
     a.sr_every = 1;
     a.nsr = 0;
@@ -360,13 +373,6 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     c->last_n = n;
     c->last_sr_interval = a.nsr > 0 ? a.sr_every * plan.strip_rows : 0;
     if (nsr_out) *nsr_out = a.nsr;
-    int32_t G = 0, T = 0;
-    int64_t P1 = 0, P2 = 0;
-    const bool refok = reference_geometry(m, n, &G, &T, &P1, &P2);
-    a.tie.mode = ((flags & SWB_FLAG_TIE_ROWMAJOR) || !refok) ? kTieRowMajor : kTieReference;
-    a.tie.G = G;
-    a.tie.T = T;
-    a.tie.C = refok ? P2 / G : 1;
 
     if ((e = cudaMemsetAsync(a.hbuf, 0xFF, sizeof(int4) * (size_t)n, c->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(a.err, 0, 4 * sizeof(int32_t), c->stream)) != cudaSuccess)

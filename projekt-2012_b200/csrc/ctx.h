@@ -83,4 +83,10 @@ int ctx_cuda_fail(swb_ctx *ctx, cudaError_t e, const char *what);
 cudaError_t ctx_get(swb_ctx *c, void *dst, const void *dev_src, size_t bytes);
 cudaError_t ctx_put(swb_ctx *c, void *dev_dst, const void *src, size_t bytes);
 
+// Rows per lane for the pair path's stage 1 (autotune.cpp): a cached choice for
+// the pair's shape bucket, else timed probes of every candidate on a slice of the
+// pair described by `base` (rows, columns, encodings, scoring and the hand-off,
+// best and error buffers must be set).  Small pairs get `fallback`.
+int autotune_rows_per_lane(swb_ctx *c, const Stage1Args &base, bool tab, bool stores, int fallback);
+
 }  // namespace swb

@@ -160,8 +160,8 @@ __global__ void presence_kernel(const uint8_t *seq, int64_t n, uint32_t *flags) 
 template <int R, bool TAB>
 cudaError_t launch_r(Stage1Args &a, const Stage1Plan &p, cudaStream_t st) {
     void *args[] = {&a};
-    const void *fn = (a.srows || a.scols) ? (const void *)stage1_kernel<R, TAB, true>
-                                          : (const void *)stage1_kernel<R, TAB, false>;
+    const void *fn = (p.stores || a.srows || a.scols) ? (const void *)stage1_kernel<R, TAB, true>
+                                                      : (const void *)stage1_kernel<R, TAB, false>;
     cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(p.blocks), dim3(kWarps * 32), args, 0, st);
     if (e != cudaSuccess) return e;
     reduce_best_kernel<<<1, 256, 0, st>>>(a.wbest, (int64_t)p.blocks * kWarps, a.best);

@@ -73,6 +73,7 @@ bool reference_geometry(int64_t rows, int64_t cols, int32_t *G, int32_t *T, int6
 // Stage-1 launch plan (chosen by the host for a pair).
 struct Stage1Plan {
     bool tab = false;      // PRMT table substitution (column alphabet of <= 4 bytes)
+    bool stores = false;   // run the store-mode kernel even without store buffers (autotuner probes)
     int R = 16;            // rows per lane
     int warps_per_block = 4;
     int blocks = 0;
