@@ -21,6 +21,7 @@
 // the best of strips run by earlier launches (the serving loop runs a pair's
 // strips over several launches).
 #include <algorithm>
+#include <cstdlib>
 #include <type_traits>
 
 #include "batch.h"
@@ -77,7 +78,7 @@ struct PairView : S {
     static constexpr int64_t *trace = nullptr;
 };
 
-template <bool TAB, class S>
+template <int R, bool TAB, class S>
 __global__ void __launch_bounds__(kWarps * 32, (std::is_same<S, NoStores>::value ? 4 : 3)) batch_kernel(BatchArgs g) {
     __shared__ int4 ring_all[kWarps][kRing];
     const int lane = threadIdx.x & 31;
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(kWarps * 32, (std::is_same<S, NoStores>::value
         b.row = 0;
         b.col = 0;
         int32_t bho = b.ho;
-        if (!run_strip<kBatchR, TAB, !std::is_same<S, NoStores>::value>(v, ring, lane, u - d.unit0, &b, bho)) {
+        if (!run_strip<R, TAB, !std::is_same<S, NoStores>::value, false>(v, ring, lane, u - d.unit0, &b, bho)) {
             if (lane == 0) {
                 atomicCAS(&g.ctl[1], kErrNone, kErrTimeout);
                 atomicExch(&g.ctl[2], 1);
@@ -197,22 +198,22 @@ __global__ void batch_encode_kernel(const uint8_t *seq, int64_t bytes, const uin
     }
 }
 
-template <bool TAB, class S>
+template <int R, bool TAB, class S>
 int max_blocks() {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_kernel<TAB, S>, kWarps * 32, 0) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_kernel<R, TAB, S>, kWarps * 32, 0) != cudaSuccess)
         return 0;
     return nb;
 }
 
-template <bool TAB, class S>
+template <int R, bool TAB, class S>
 cudaError_t launch(const BatchArgs &a, int sms, int cap, cudaStream_t st) {
-    const int per_sm = std::max(1, max_blocks<TAB, S>());
+    const int per_sm = std::max(1, max_blocks<R, TAB, S>());
     const int64_t need = (a.nunits + kWarps - 1) / kWarps;
     int64_t limit = (int64_t)per_sm * sms;
     if (cap > 0 && cap < limit) limit = cap;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(need, limit));
-    batch_kernel<TAB, S><<<blocks, kWarps * 32, 0, st>>>(a);
+    batch_kernel<R, TAB, S><<<blocks, kWarps * 32, 0, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -222,34 +223,50 @@ cudaError_t batch_configure() {
     const int c = cudaSharedmemCarveoutMaxShared;
     const auto A = cudaFuncAttributePreferredSharedMemoryCarveout;
     cudaError_t e = cudaSuccess;
-    for (cudaError_t x : {cudaFuncSetAttribute((const void *)batch_kernel<false, NoStores>, A, c),
-                          cudaFuncSetAttribute((const void *)batch_kernel<true, NoStores>, A, c),
-                          cudaFuncSetAttribute((const void *)batch_kernel<false, WithStores>, A, c),
-                          cudaFuncSetAttribute((const void *)batch_kernel<true, WithStores>, A, c),
-                          cudaFuncSetAttribute((const void *)batch_kernel<false, WithBounds>, A, c),
-                          cudaFuncSetAttribute((const void *)batch_kernel<true, WithBounds>, A, c),
+    for (cudaError_t x : {cudaFuncSetAttribute((const void *)batch_kernel<8, false, NoStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_kernel<8, true, NoStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_kernel<16, false, NoStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_kernel<16, true, NoStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_kernel<16, false, WithStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_kernel<16, true, WithStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_kernel<16, false, WithBounds>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_kernel<16, true, WithBounds>, A, c),
                           cudaFuncSetAttribute((const void *)batch_reduce_kernel, A, c),
                           cudaFuncSetAttribute((const void *)batch_encode_kernel, A, c)})
         if (x != cudaSuccess) e = x;
     return e;
 }
 
-int batch_max_blocks_per_sm(bool tab, BatchMode mode) {
-    if (mode == kBatchBounds) return tab ? max_blocks<true, WithBounds>() : max_blocks<false, WithBounds>();
-    if (mode == kBatchStores) return tab ? max_blocks<true, WithStores>() : max_blocks<false, WithStores>();
-    return tab ? max_blocks<true, NoStores>() : max_blocks<false, NoStores>();
+int batch_score_rows_per_lane() {
+    // measured on the 100,000-pair batch: R = 16 299 ms, R = 8 413 ms
+    if (const char *v = std::getenv("SWB_BATCH_R")) {
+        const int r = std::atoi(v);
+        if (r == 8 || r == 16) return r;
+    }
+    return 16;
 }
 
-cudaError_t batch_launch(const BatchArgs &a, bool tab, BatchMode mode, int sms, int max_blocks, int64_t npairs,
+int batch_max_blocks_per_sm(bool tab, BatchMode mode) {
+    if (mode == kBatchBounds) return tab ? max_blocks<16, true, WithBounds>() : max_blocks<16, false, WithBounds>();
+    if (mode == kBatchStores) return tab ? max_blocks<16, true, WithStores>() : max_blocks<16, false, WithStores>();
+    return tab ? max_blocks<16, true, NoStores>() : max_blocks<16, false, NoStores>();
+}
+
+cudaError_t batch_launch(const BatchArgs &a, bool tab, BatchMode mode, int R, int sms, int max_blocks, int64_t npairs,
                          BestRec *pbest, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
     if (a.nunits > 0) {
         if (mode == kBatchBounds)
-            e = tab ? launch<true, WithBounds>(a, sms, max_blocks, st) : launch<false, WithBounds>(a, sms, max_blocks, st);
+            e = tab ? launch<16, true, WithBounds>(a, sms, max_blocks, st)
+                    : launch<16, false, WithBounds>(a, sms, max_blocks, st);
         else if (mode == kBatchStores)
-            e = tab ? launch<true, WithStores>(a, sms, max_blocks, st) : launch<false, WithStores>(a, sms, max_blocks, st);
+            e = tab ? launch<16, true, WithStores>(a, sms, max_blocks, st)
+                    : launch<16, false, WithStores>(a, sms, max_blocks, st);
+        else if (R == 8)
+            e = tab ? launch<8, true, NoStores>(a, sms, max_blocks, st) : launch<8, false, NoStores>(a, sms, max_blocks, st);
         else
-            e = tab ? launch<true, NoStores>(a, sms, max_blocks, st) : launch<false, NoStores>(a, sms, max_blocks, st);
+            e = tab ? launch<16, true, NoStores>(a, sms, max_blocks, st)
+                    : launch<16, false, NoStores>(a, sms, max_blocks, st);
         if (e != cudaSuccess) return e;
     }
     if (npairs > 0) {

@@ -53,8 +53,8 @@ struct BatchArgs {
     int2 *srows, *scols;       // store pass: special rows (H, F) / columns (H, E) of every pair
 };
 
-// Rows per lane of the batched kernel (its strips are 32 * kBatchR rows; the
-// store pass relies on 512-row strips for the walker's grid).
+// Rows per lane of the batched kernel's store passes (their strips are 512 rows,
+// the walker's block height); score-only passes may use 8 (256-row strips).
 constexpr int kBatchR = 16;
 constexpr int kBatchStripRows = 32 * kBatchR;
 
@@ -65,13 +65,15 @@ constexpr int kBatchStripRows = 32 * kBatchR;
 // same launch's unit order or finished by an earlier launch.  `mode` selects
 // what is stored.  max_blocks > 0 caps the grid (the rest of the GPU stays free
 // for other work).
-cudaError_t batch_launch(const BatchArgs &a, bool tab, BatchMode mode, int sms, int max_blocks, int64_t npairs,
-                         BestRec *pbest, cudaStream_t st);
+cudaError_t batch_launch(const BatchArgs &a, bool tab, BatchMode mode, int R, int sms, int max_blocks,
+                         int64_t npairs, BestRec *pbest, cudaStream_t st);
 // Byte presence flags over a buffer (TAB-mode choice) and the TAB encodings of
 // every byte of seq (rcode[i] = lut[seq[i]], ctab[i] = table word of seq[i]).
 cudaError_t batch_encode(const uint8_t *seq, int64_t bytes, const uint8_t *d_lut, uint8_t *rcode, uint32_t *ctab,
                          int32_t mt1, int32_t mm1, uint32_t *tab_hi, cudaStream_t st);
 int batch_max_blocks_per_sm(bool tab, BatchMode mode);
+// Rows per lane of score-only batched launches (16 unless SWB_BATCH_R overrides).
+int batch_score_rows_per_lane();
 
 // Host batch with every pair traced, in one scoring pass that keeps the stores
 // (the serving loop's iteration).  Same contract as swb_batch_align(..., 1.0, ...).

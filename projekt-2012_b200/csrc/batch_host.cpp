@@ -26,7 +26,8 @@ struct PairInfo {
 // Lays out the units of `order` (indices into info, already sorted) as one
 // launch: unit0 / ufirst / ucount / hbuf offsets; returns the unit count.
 int64_t layout_units(const std::vector<PairInfo> &info, const std::vector<int64_t> &order, uint32_t flags,
-                     std::vector<BatchPair> &bp, std::vector<int32_t> &unit_pair, int64_t *hbuf_entries) {
+                     int strip_rows, std::vector<BatchPair> &bp, std::vector<int32_t> &unit_pair,
+                     int64_t *hbuf_entries) {
     bp.resize(order.size());
     unit_pair.clear();
     int64_t units = 0, hb = 0;
@@ -38,7 +39,7 @@ int64_t layout_units(const std::vector<PairInfo> &info, const std::vector<int64_
         d.col_off = p.col_off;
         d.m = (int32_t)p.m;
         d.n = (int32_t)p.n;
-        d.nstrips = (int32_t)((p.m + kBatchStripRows - 1) / kBatchStripRows);
+        d.nstrips = (int32_t)((p.m + strip_rows - 1) / strip_rows);
         d.unit0 = (int32_t)units;
         d.ufirst = (int32_t)units;
         d.ucount = d.nstrips;
@@ -66,7 +67,7 @@ int64_t layout_units(const std::vector<PairInfo> &info, const std::vector<int64_
 // Runs one scoring launch (optionally the store pass) over bp; pbest receives
 // one record per entry of bp (slot k).
 int run_launch(swb_ctx *c, const uint8_t *d_seq, bool tab, const BatchArgs &base, std::vector<BatchPair> &bp,
-               std::vector<int32_t> &unit_pair, int64_t hbuf_entries, bool stores, std::vector<BestRec> &pbest,
+               std::vector<int32_t> &unit_pair, int64_t hbuf_entries, bool stores, int R, std::vector<BestRec> &pbest,
                float *ms) {
     cudaError_t e;
     const int64_t np = (int64_t)bp.size(), nu = (int64_t)unit_pair.size();
@@ -103,7 +104,7 @@ int run_launch(swb_ctx *c, const uint8_t *d_seq, bool tab, const BatchArgs &base
         (e = cudaMemsetAsync(a.ctl, 0, 4 * sizeof(int32_t), c->stream)) != cudaSuccess)
         return ctx_cuda_fail(c, e, "batch set-up");
     cudaEventRecord(c->ev0, c->stream);
-    if ((e = batch_launch(a, tab, stores ? kBatchStores : kBatchScore, c->sms, c->max_blocks, np,
+    if ((e = batch_launch(a, tab, stores ? kBatchStores : kBatchScore, R, c->sms, c->max_blocks, np,
                           (BestRec *)c->b_pbest.p, c->stream)) !=
         cudaSuccess)
         return ctx_cuda_fail(c, e, "batch launch");
@@ -259,8 +260,9 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
     std::vector<BestRec> pbest;
     int64_t hb = 0, srn = 0, scn = 0, ops_total = 0, xp_total = 0;
     float ms1 = 0.f;
-    layout_units(info, order, flags, bp, unit_pair, &hb);
     const bool first_stores = stores_first && !order.empty();
+    const int R1 = first_stores ? kBatchR : batch_score_rows_per_lane();
+    layout_units(info, order, flags, 32 * R1, bp, unit_pair, &hb);
     if (!order.empty()) {
         BatchArgs a1 = base;
         if (first_stores) {
@@ -270,7 +272,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
             a1.srows = (int2 *)c->b_srows.p;
             a1.scols = (int2 *)c->b_scols.p;
         }
-        int rc = run_launch(c, d_seq, tab, a1, bp, unit_pair, hb, first_stores, pbest, &ms1);
+        int rc = run_launch(c, d_seq, tab, a1, bp, unit_pair, hb, first_stores, R1, pbest, &ms1);
         if (rc != SWB_OK) return rc;
         launches += 2;
     }
@@ -317,7 +319,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
             // strip), special columns every 256 columns
             std::vector<int32_t> up2;
             int64_t hb2 = 0;
-            layout_units(info, tr, flags, bpw, up2, &hb2);
+            layout_units(info, tr, flags, kBatchStripRows, bpw, up2, &hb2);
             layout_stores(bpw, out->items, tr, &srn, &scn, &ops_total, &xp_total);
             int rc = ensure_stores(srn, scn);
             if (rc != SWB_OK) return rc;
@@ -326,7 +328,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
             b2.scols = (int2 *)c->b_scols.p;
             std::vector<BestRec> pb2;
             float ms2 = 0.f;
-            rc = run_launch(c, d_seq, tab, b2, bpw, up2, hb2, true, pb2, &ms2);
+            rc = run_launch(c, d_seq, tab, b2, bpw, up2, hb2, true, kBatchR, pb2, &ms2);
             if (rc != SWB_OK) return rc;
             launches += 2;
             for (size_t k = 0; k < tr.size(); ++k) {

@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(kWarps * 32, (R <= 16 ? 4 : 2)) stage1_kernel(
             asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
             a.trace[3 * s + 2] = (int64_t)smid;
         }
-        if (!run_strip<R, TAB, STORES>(a, ring, lane, (int32_t)s, &b, bho)) failed = true;
+        if (!run_strip<R, TAB, STORES, !STORES>(a, ring, lane, (int32_t)s, &b, bho)) failed = true;
         if (a.trace && lane == 0) {
             unsigned long long t;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

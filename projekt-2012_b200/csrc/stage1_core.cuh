@@ -285,9 +285,10 @@ __device__ __forceinline__ bool refill(const A &a, int4 *ring, int lane, int32_t
 }
 
 // STORES: the launch may write special rows or columns (a.srows or a.scols set).
-// Kernels are instantiated per mode so that each holds only the step bodies it
-// runs (the step loop's speed depends on what else is compiled into it).
-template <int R, bool TAB, bool STORES, class A>
+// UNROLL: unroll the score-only chunk (used when STORES is false).  Kernels are
+// instantiated per mode so that each holds only the step bodies it runs (the
+// step loop's speed depends on what else is compiled into it).
+template <int R, bool TAB, bool STORES, bool UNROLL, class A>
 __device__ bool run_strip(const A &a, int4 *ring, int lane, int32_t s, Best *b, int32_t &bho) {
     Lane<R> L;
     StripCtx sc;
@@ -372,11 +373,15 @@ __device__ bool run_strip(const A &a, int4 *ring, int lane, int32_t s, Best *b, 
         // lane l stores special column j = q*sc_every - 1 at step j + l: a chunk of
         // steps [k, k+kCH) needs the check when some (t + 1) mod sc_every < 32
         const bool sc_window = a.scols != nullptr && ((k + kCH) & (a.sc_every - 1)) < 32 + kCH;
-        // Score-only launches run an unrolled chunk; launches with stores keep
-        // their chunks rolled (measured on the 1 Mbp pair: unrolling the scoring
-        // chunk saves about 8%, unrolled chunks with stores cost 20-130%).
-        if constexpr (!STORES) {
+        // Score-only launches of the pair kernel run an unrolled chunk; the
+        // batched kernel and launches with stores keep their chunks rolled
+        // (measured: unrolling saves about 8% of the pair kernel's score-only
+        // time on the 1 Mbp pair, but costs the batched kernel about 50% and
+        // chunks with stores 20-130%).
+        if constexpr (!STORES && UNROLL) {
 #pragma unroll
+            for (int u = 0; u < kCH; ++u) step<R, TAB, false, false, false>(L, a, b, ring, lane, sc, k + u);
+        } else if constexpr (!STORES) {
             for (int u = 0; u < kCH; ++u) step<R, TAB, false, false, false>(L, a, b, ring, lane, sc, k + u);
         } else if (sc_window) {
             for (int u = 0; u < kCH; ++u) step<R, TAB, false, true, true>(L, a, b, ring, lane, sc, k + u);

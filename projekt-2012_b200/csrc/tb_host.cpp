@@ -181,7 +181,7 @@ int traceback(cudaStream_t st, int sms, const uint8_t *d_rows, int64_t m, const 
                 (e = cudaMemsetAsync(dg, 0, sizeof(int32_t) * (size_t)ncell, st)) != cudaSuccess ||
                 (e = cudaMemsetAsync(dpb, 0, sizeof(BestRec) * (size_t)ncell, st)) != cudaSuccess ||
                 (e = cudaMemsetAsync(dc, 0, 4 * sizeof(int32_t), st)) != cudaSuccess ||
-                (e = batch_launch(ba, false, kBatchBounds, sms, 0, ncell, dpb, st)) != cudaSuccess) {
+                (e = batch_launch(ba, false, kBatchBounds, kBatchR, sms, 0, ncell, dpb, st)) != cudaSuccess) {
                 err = std::string("level-1 recompute: ") + cudaGetErrorString(e);
                 return SWB_ECUDA;
             }
