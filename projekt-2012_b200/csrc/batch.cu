@@ -80,10 +80,11 @@ struct PairView : S {
 
 template <int R, bool TAB, class S>
 __global__ void __launch_bounds__(kWarps * 32, (std::is_same<S, NoStores>::value ? 4 : 3)) batch_kernel(BatchArgs g) {
-    __shared__ int4 ring_all[kWarps][kRing];
+    __shared__ int4 ring_all[kWarps][kRing + kStage];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     int4 *ring = ring_all[wib];
+    int4 *stage = ring + kRing;
     for (;;) {
         __syncwarp();
         int32_t u = 0;
@@ -125,7 +126,7 @@ __global__ void __launch_bounds__(kWarps * 32, (std::is_same<S, NoStores>::value
         b.row = 0;
         b.col = 0;
         int32_t bho = b.ho;
-        if (!run_strip<R, TAB, !std::is_same<S, NoStores>::value, false>(v, ring, lane, u - d.unit0, &b, bho)) {
+        if (!run_strip<R, TAB, !std::is_same<S, NoStores>::value, false>(v, ring, stage, lane, u - d.unit0, &b, bho)) {
             if (lane == 0) {
                 atomicCAS(&g.ctl[1], kErrNone, kErrTimeout);
                 atomicExch(&g.ctl[2], 1);

@@ -52,10 +52,11 @@ namespace {
 
 template <int R, bool TAB, bool STORES>
 __global__ void __launch_bounds__(kWarps * 32, (R <= 16 ? 4 : 2)) stage1_kernel(Stage1Args a) {
-    __shared__ int4 ring_all[kWarps][kRing];
+    __shared__ int4 ring_all[kWarps][kRing + kStage];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     int4 *ring = ring_all[wib];
+    int4 *stage = ring + kRing;
     const int64_t B = gridDim.x;
 
     Best b;
@@ -73,7 +74,7 @@ __global__ void __launch_bounds__(kWarps * 32, (R <= 16 ? 4 : 2)) stage1_kernel(
             asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
             a.trace[3 * s + 2] = (int64_t)smid;
         }
-        if (!run_strip<R, TAB, STORES, !STORES>(a, ring, lane, (int32_t)s, &b, bho)) failed = true;
+        if (!run_strip<R, TAB, STORES, !STORES>(a, ring, stage, lane, (int32_t)s, &b, bho)) failed = true;
         if (a.trace && lane == 0) {
             unsigned long long t;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

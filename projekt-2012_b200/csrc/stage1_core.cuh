@@ -25,6 +25,7 @@ namespace {
 
 constexpr int kCH = 8;         // steps per refill
 constexpr int kRing = 32;      // ring entries per warp
+constexpr int kStage = 16;     // staged bottom-row entries per warp (flushed every refill)
 constexpr int kWarps = 4;      // warps per block
 constexpr long long kWaitLimitCycles = 40LL * 1000 * 1000 * 1000;  // bound of every wait (~20 s)
 
@@ -122,8 +123,10 @@ struct StripCtx {
 };
 
 // One anti-diagonal step.  PRED: some lanes of the warp are outside [0, n).
-// SC: this step may be a special-column step of some lane.  SR: the strip's
-// bottom row may be a special row (when false the store is compiled out).
+// SC: this step may be a special-column step of some lane.  Lane 31 stages the
+// strip's bottom row {H + open, F below, F, -} for its column in shared memory;
+// the refill writes the staged columns out (hand-off buffer, special row), so
+// the step itself issues no global store.
 //
 // Phase 1 computes, for every row of the lane, E and t = max(H_diag + s, E, 0)
 // (independent of the vertical chain); phase 2 runs the F chain and writes HO.
@@ -131,8 +134,8 @@ struct StripCtx {
 // copies are needed.  The column maximum is taken over t: a cell whose H comes
 // from F is strictly below the cell above it, so it can never hold the best
 // score, and a best cell always has H = t.
-template <int R, bool TAB, bool PRED, bool SC, bool SR, class A>
-__device__ __forceinline__ void step(Lane<R> &L, const A &a, Best *b, const int4 *ring, int lane,
+template <int R, bool TAB, bool PRED, bool SC, class A>
+__device__ __forceinline__ void step(Lane<R> &L, const A &a, Best *b, const int4 *ring, int4 *stage, int lane,
                                      const StripCtx &sc, int32_t k) {
     const int32_t j = k - lane;
     const bool act = !PRED || (j >= 0 && j < sc.n);
@@ -183,10 +186,7 @@ __device__ __forceinline__ void step(Lane<R> &L, const A &a, Best *b, const int4
     // outputs toward the lane below; lane 31 hands its slot to lane 0
     const int4 rv = ring[(k + 1) & (kRing - 1)];
     const bool last = (lane == 31);
-    if (last && act) {
-        if (sc.below) st_ll(a.hbuf + j, L.HO[R - 1], f, sc.strip);
-        if (SR && sc.sr) a.srows[sc.sr_off + j] = make_int2(L.HO[R - 1] - a.open, flast);
-    }
+    if (last && act) stage[j & (kStage - 1)] = make_int4(L.HO[R - 1], f, flast, 0);
     const int32_t oHO = last ? rv.x : L.HO[R - 1];
     const int32_t oF = last ? rv.y : f;
     const uint32_t oB = last ? (uint32_t)rv.z : cb;
@@ -264,9 +264,28 @@ __device__ __forceinline__ bool commit(const A &a, int4 *ring, int32_t strip, in
 
 // Refill at step k (k % kCH == 0): lanes 0..kCH-1 commit columns [k+kCH, k+2kCH)
 // (prefetched one refill ago) and prefetch columns [k+2kCH, k+3kCH).
+// Writes out the bottom-row columns lane 31 staged in the 8 steps before step k:
+// columns [k - kCH - 31, k - 31) (lanes 0..kCH-1, one column each): the
+// hand-off entry for the strip below and, for a special row, (H, F).
+template <class A>
+__device__ __forceinline__ void flush(const A &a, const int4 *stage, int lane, const StripCtx &sc, int32_t n,
+                                      int32_t k) {
+    __syncwarp();
+    if (lane < kCH && (sc.below || sc.sr)) {
+        const int32_t c = k - kCH - 31 + lane;
+        if (c >= 0 && c < n) {
+            const int4 v = stage[c & (kStage - 1)];
+            if (sc.below) st_ll(a.hbuf + c, v.x, v.y, sc.strip);
+            if (sc.sr) a.srows[sc.sr_off + c] = make_int2(v.x - a.open, v.z);
+        }
+    }
+}
+
 template <bool TAB, class A>
-__device__ __forceinline__ bool refill(const A &a, int4 *ring, int lane, int32_t strip, int32_t n,
-                                       int32_t k, Pre &pre, int32_t &thr, int32_t bho, int32_t &gpre) {
+__device__ __forceinline__ bool refill(const A &a, int4 *ring, const int4 *stage, int lane, const StripCtx &sc,
+                                       int32_t n, int32_t k, Pre &pre, int32_t &thr, int32_t bho, int32_t &gpre) {
+    const int32_t strip = sc.strip;
+    flush(a, stage, lane, sc, n, k);
     // cells below the best H found anywhere so far can never win: raise the
     // candidate threshold to it (ties at that value are still examined); the
     // value was loaded one refill ago
@@ -285,11 +304,11 @@ __device__ __forceinline__ bool refill(const A &a, int4 *ring, int lane, int32_t
 }
 
 // STORES: the launch may write special rows or columns (a.srows or a.scols set).
-// UNROLL: unroll the score-only chunk (used when STORES is false).  Kernels are
-// instantiated per mode so that each holds only the step bodies it runs (the
-// step loop's speed depends on what else is compiled into it).
+// UNROLL: unroll the plain 8-step chunks.  Kernels are instantiated per mode so
+// that each holds only the step bodies it runs (the step loop's speed depends on
+// what else is compiled into it).
 template <int R, bool TAB, bool STORES, bool UNROLL, class A>
-__device__ bool run_strip(const A &a, int4 *ring, int lane, int32_t s, Best *b, int32_t &bho) {
+__device__ bool run_strip(const A &a, int4 *ring, int4 *stage, int lane, int32_t s, Best *b, int32_t &bho) {
     Lane<R> L;
     StripCtx sc;
     const int64_t H = 32LL * R;
@@ -363,39 +382,39 @@ __device__ bool run_strip(const A &a, int4 *ring, int lane, int32_t s, Best *b, 
     if (n > 32) kB = 32 + ((n - 32) / kCH) * kCH;
     int32_t k = 0;
     for (; k < kA; ++k) {
-        if (k > 0 && (k % kCH) == 0 && !refill<TAB>(a, ring, lane, s, n, k, pre, L.thr, L.bho, gpre)) return false;
-        if constexpr (!STORES) step<R, TAB, true, false, false>(L, a, b, ring, lane, sc, k);
-        else if (a.scols) step<R, TAB, true, true, true>(L, a, b, ring, lane, sc, k);
-        else step<R, TAB, true, false, true>(L, a, b, ring, lane, sc, k);
+        if (k > 0 && (k % kCH) == 0 && !refill<TAB>(a, ring, stage, lane, sc, n, k, pre, L.thr, L.bho, gpre)) return false;
+        if constexpr (!STORES) step<R, TAB, true, false>(L, a, b, ring, stage, lane, sc, k);
+        else if (a.scols) step<R, TAB, true, true>(L, a, b, ring, stage, lane, sc, k);
+        else step<R, TAB, true, false>(L, a, b, ring, stage, lane, sc, k);
     }
     while (k < kB) {
-        if (!refill<TAB>(a, ring, lane, s, n, k, pre, L.thr, L.bho, gpre)) return false;
+        if (!refill<TAB>(a, ring, stage, lane, sc, n, k, pre, L.thr, L.bho, gpre)) return false;
         // lane l stores special column j = q*sc_every - 1 at step j + l: a chunk of
         // steps [k, k+kCH) needs the check when some (t + 1) mod sc_every < 32
         const bool sc_window = a.scols != nullptr && ((k + kCH) & (a.sc_every - 1)) < 32 + kCH;
-        // Score-only launches of the pair kernel run an unrolled chunk; the
-        // batched kernel and launches with stores keep their chunks rolled
-        // (measured: unrolling saves about 8% of the pair kernel's score-only
-        // time on the 1 Mbp pair, but costs the batched kernel about 50% and
-        // chunks with stores 20-130%).
-        if constexpr (!STORES && UNROLL) {
+        // The pair kernel's score-only launches unroll the chunk; the batched
+        // kernel and launches with stores keep it rolled (measured on the 1 Mbp
+        // pair: unrolling saves 5-8% of the score-only time but costs the
+        // store-mode kernel 27% and the batched kernel about 50%).
+        if (STORES && sc_window) {
+            for (int u = 0; u < kCH; ++u) step<R, TAB, false, true>(L, a, b, ring, stage, lane, sc, k + u);
+        } else if constexpr (UNROLL) {
 #pragma unroll
-            for (int u = 0; u < kCH; ++u) step<R, TAB, false, false, false>(L, a, b, ring, lane, sc, k + u);
-        } else if constexpr (!STORES) {
-            for (int u = 0; u < kCH; ++u) step<R, TAB, false, false, false>(L, a, b, ring, lane, sc, k + u);
-        } else if (sc_window) {
-            for (int u = 0; u < kCH; ++u) step<R, TAB, false, true, true>(L, a, b, ring, lane, sc, k + u);
+            for (int u = 0; u < kCH; ++u) step<R, TAB, false, false>(L, a, b, ring, stage, lane, sc, k + u);
         } else {
-            for (int u = 0; u < kCH; ++u) step<R, TAB, false, false, true>(L, a, b, ring, lane, sc, k + u);
+            for (int u = 0; u < kCH; ++u) step<R, TAB, false, false>(L, a, b, ring, stage, lane, sc, k + u);
         }
         k += kCH;
     }
     for (; k < kEnd; ++k) {
-        if ((k % kCH) == 0 && !refill<TAB>(a, ring, lane, s, n, k, pre, L.thr, L.bho, gpre)) return false;
-        if constexpr (!STORES) step<R, TAB, true, false, false>(L, a, b, ring, lane, sc, k);
-        else if (a.scols) step<R, TAB, true, true, true>(L, a, b, ring, lane, sc, k);
-        else step<R, TAB, true, false, true>(L, a, b, ring, lane, sc, k);
+        if ((k % kCH) == 0 && !refill<TAB>(a, ring, stage, lane, sc, n, k, pre, L.thr, L.bho, gpre)) return false;
+        if constexpr (!STORES) step<R, TAB, true, false>(L, a, b, ring, stage, lane, sc, k);
+        else if (a.scols) step<R, TAB, true, true>(L, a, b, ring, stage, lane, sc, k);
+        else step<R, TAB, true, false>(L, a, b, ring, stage, lane, sc, k);
     }
+    // the columns staged since the last refill
+    flush(a, stage, lane, sc, n, ((kEnd + kCH - 1) / kCH) * kCH);
+    __syncwarp();
     bho = L.bho;
     return true;
 }
