@@ -41,6 +41,7 @@ def parse_args():
     p.add_argument("--no-mixed", action="store_true", help="skip the batched and serving measurements")
     p.add_argument("--batch-pairs", type=int, default=100_000, help="pairs of the batched workload")
     p.add_argument("--serve-seconds", type=float, default=20.0, help="length of the Poisson serving run")
+    p.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
     return p.parse_args()
 
 
@@ -427,7 +428,7 @@ def main():
     if not args.no_mixed:
         ctx.close()
         mixed_batched = batched_metrics(args, local)
-        mixed_serving = serving_metrics(args, local)
+        mixed_serving = None if args.no_serving else serving_metrics(args, local)
     d2h = 64 + first.n_ops + 24 * len(first.xpoints)
     line = {
         "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
