@@ -244,6 +244,32 @@ def batched_metrics(args, device):
         p = ctx.align(buf[ao:ao + al].tobytes(), buf[bo:bo + bl].tobytes(), sc, swb200.FLAG_SCORE_ONLY)
         assert (p.score, p.end_row, p.end_col) == (r.score[i], r.end_row[i], r.end_col[i])
     plain = len(sample) / (time.perf_counter() - t0)
+    # per-call cost of a serving-sized batch (32 pairs of 300-700 bp, every pair
+    # traced): one replayed CUDA graph against the same kernels launched directly
+    srng = np.random.default_rng(5)
+    parts, srefs, off = [], [], 0
+    for _ in range(32):
+        la, lb = int(srng.integers(300, 700)), int(srng.integers(300, 700))
+        a = srng.choice(np.frombuffer(b"ACGT", np.uint8), la)
+        b = np.concatenate([a[: lb // 2], srng.choice(np.frombuffer(b"ACGT", np.uint8), lb - lb // 2)])
+        parts += [a, b]
+        srefs.append((off, la, off + la, lb))
+        off += la + lb
+    sbuf = np.concatenate(parts)
+    srefs = np.array(srefs, dtype=np.int64)
+    small = {}
+    for mode in ("1", "0"):
+        os.environ["SWB_BATCH_GRAPH"] = mode
+        for _ in range(5):
+            ctx.batch_align(sbuf, srefs, sc, trace_frac=1.0)
+        ts = []
+        for _ in range(60):
+            t0 = time.perf_counter()
+            rs = ctx.batch_align(sbuf, srefs, sc, trace_frac=1.0)
+            ts.append((time.perf_counter() - t0) * 1e3)
+        ts.sort()
+        small[mode] = (ts[len(ts) // 2], rs.kernel_launches)
+    os.environ.pop("SWB_BATCH_GRAPH", None)
     ctx.close()
     n = len(refs)
     return {"workload": f"{n} pairs, query clip(round(lognormal(ln 1000, 0.75)), 100, 10000), target 1.5x "
@@ -253,7 +279,11 @@ def batched_metrics(args, device):
             "stage1_ms": min(x[1] for x in runs), "stage2_ms": min(x[2] for x in runs),
             "kernel_launches": runs[-1][3], "plain_pairs_per_s": plain, "vs_plain": n / wall / plain,
             "plain_sample": f"{len(sample)} pairs of the same batch through swb_align_pair, score only, equal results",
-            "timing": "wall clock of swb_batch_align from host memory (host->device copy, results back)"}
+            "timing": "wall clock of swb_batch_align from host memory (host->device copy, results back)",
+            "small_batch": {"workload": "32 pairs of 300-700 bp, every pair traced (a serving iteration's size)",
+                            "graph_ms_p50": small["1"][0], "graph_kernels": small["1"][1],
+                            "direct_ms_p50": small["0"][0], "direct_kernels": small["0"][1],
+                            "timing": "wall clock per swb_batch_align call, median of 60"}}
 
 
 def serving_metrics(args, device):

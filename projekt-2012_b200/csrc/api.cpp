@@ -163,6 +163,7 @@ int swb_ctx_create(const swb_options *opts, swb_ctx **out) {
         (c->opts.cuda_stream == 0 &&
          (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) ||
         (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess ||
+        (e = cudaEventCreate(&c->ev2)) != cudaSuccess ||
         (e = swb::stage1_configure()) != cudaSuccess || (e = swb::batch_configure()) != cudaSuccess ||
         (e = swb::tb::walker_configure()) != cudaSuccess) {
         int rc = ctx_cuda_fail(nullptr, e, "swb_ctx_create");
@@ -186,8 +187,14 @@ void swb_ctx_destroy(swb_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->h_stage.release();
     c->h_io.release();
+    c->h_gin.release();
+    c->h_gout.release();
+    for (auto &g : c->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->ev2) cudaEventDestroy(c->ev2);
     if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
 }

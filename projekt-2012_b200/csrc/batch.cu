@@ -78,8 +78,9 @@ struct PairView : S {
     static constexpr int64_t *trace = nullptr;
 };
 
+// Claims units until the queue is empty and runs each as one strip.
 template <int R, bool TAB, class S>
-__global__ void __launch_bounds__(kWarps * 32, (std::is_same<S, NoStores>::value ? 4 : 3)) batch_kernel(BatchArgs g) {
+__device__ __forceinline__ void batch_body(const BatchArgs &g) {
     __shared__ int4 ring_all[kWarps][kRing + kStage];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -158,16 +159,27 @@ __global__ void __launch_bounds__(kWarps * 32, (std::is_same<S, NoStores>::value
     }
 }
 
+template <int R, bool TAB, class S>
+__global__ void __launch_bounds__(kWarps * 32, (std::is_same<S, NoStores>::value ? 4 : 3)) batch_kernel(BatchArgs g) {
+    batch_body<R, TAB, S>(g);
+}
+
+// The graphed form: arguments from the call's header; the instance of the
+// other mode returns at once.
+template <int R, bool TAB, class S>
+__global__ void __launch_bounds__(kWarps * 32, (std::is_same<S, NoStores>::value ? 4 : 3))
+    batch_graph_kernel(const GraphHdr *h) {
+    if ((h->tab != 0) != TAB) return;
+    const BatchArgs g = h->ba;
+    batch_body<R, TAB, S>(g);
+}
+
 __device__ __forceinline__ void merge(BestRec &b, const BestRec &r) {
     if (r.valid && (!b.valid || better(r.ho, r.key, b.ho, b.key))) b = r;
 }
 
-// A warp per pair: merges the pair's units of this launch into pbest[slot].
-__global__ void batch_reduce_kernel(const BatchPair *pairs, int64_t npairs, const BestRec *ubest, BestRec *pbest) {
-    const int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (p >= npairs) return;
-    const BatchPair d = pairs[p];
+// Merges the units of pair d of this launch into pbest[d.slot] (one warp).
+__device__ __forceinline__ void reduce_pair(const BatchPair &d, int lane, const BestRec *ubest, BestRec *pbest) {
     BestRec b;
     b.ho = INT_MIN;
     b.valid = 0;
@@ -187,6 +199,98 @@ __global__ void batch_reduce_kernel(const BatchPair *pairs, int64_t npairs, cons
         merge(b, o);
     }
     if (lane == 0) pbest[d.slot] = b;
+}
+
+// A warp per pair: merges the pair's units of this launch into pbest[slot].
+__global__ void batch_reduce_kernel(const BatchPair *pairs, int64_t npairs, const BestRec *ubest, BestRec *pbest) {
+    const int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (p >= npairs) return;
+    reduce_pair(pairs[p], threadIdx.x & 31, ubest, pbest);
+}
+
+__global__ void graph_reduce_kernel(const GraphHdr *h) {
+    const int64_t np = h->npairs;
+    const BatchPair *pairs = h->ba.pairs;
+    const BestRec *ubest = h->ba.ubest;
+    BestRec *pbest = h->pbest;
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += warps)
+        reduce_pair(pairs[p], threadIdx.x & 31, ubest, pbest);
+}
+
+// Graph step 1: resets the launch's control words, per-pair bests and hand-off
+// entries, and ORs the byte values of the sequences into the presence bitmap
+// (which the decide kernel clears again after reading it).
+__global__ void graph_prepare_kernel(const GraphHdr *h) {
+    __shared__ uint32_t sh[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int32_t *ctl = h->out;
+    if (tid < 4) ctl[tid] = 0;
+    int4 *hbuf = h->ba.hbuf;
+    for (int64_t i = tid, e = h->hbuf_entries; i < e; i += stride) hbuf[i] = make_int4(-1, -1, -1, -1);
+    int32_t *gbest = h->ba.gbest;
+    BestRec *pbest = h->pbest;
+    for (int64_t i = tid, e = h->npairs; i < e; i += stride) {
+        gbest[i] = 0;
+        BestRec z;
+        z.ho = 0;
+        z.valid = 0;
+        z.key = 0;
+        z.row = 0;
+        z.col = 0;
+        pbest[i] = z;
+    }
+    if (h->tab_ok) {
+        const uint8_t *seq = h->ba.seq;
+        for (int64_t i = tid, e = h->seq_bytes; i < e; i += stride) sh[seq[i]] = 1;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+        if (sh[i]) atomicOr(&h->presence[i >> 5], 1u << (i & 31));
+}
+
+// Graph step 2 (one block of 256 threads, thread = byte value): the table path
+// when at most four byte values occur; codes in byte order, 7 for absent bytes.
+__global__ void graph_decide_kernel(GraphHdr *h) {
+    __shared__ uint32_t bits[8];
+    const int b = threadIdx.x;
+    if (b < 8) bits[b] = h->presence[b];
+    __syncthreads();
+    if (b < 8) h->presence[b] = 0;
+    int total = 0, below = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        total += __popc(bits[k]);
+        if (k < (b >> 5)) below += __popc(bits[k]);
+    }
+    const uint32_t w = bits[b >> 5];
+    below += __popc(w & ((1u << (b & 31)) - 1u));
+    const bool present = (w >> (b & 31)) & 1u;
+    const int tab = (h->tab_ok && total <= 4) ? 1 : 0;
+    h->lut[b] = present ? (uint8_t)below : (uint8_t)7;
+    if (b == 0) {
+        h->tab = tab;
+        h->out[4] = tab;
+    }
+}
+
+// Graph step 3: table encodings of every byte (table path only).
+__global__ void graph_encode_kernel(const GraphHdr *h) {
+    if (!h->tab) return;
+    const uint8_t *seq = h->ba.seq;
+    const uint8_t *lut = h->lut;
+    uint8_t *rcode = const_cast<uint8_t *>(h->ba.rcode);
+    uint32_t *ctab = const_cast<uint32_t *>(h->ba.ctab);
+    const uint32_t mm4 = h->ba.tab_hi, x1 = h->x1;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, e = h->seq_bytes; i < e; i += stride) {
+        const uint32_t q = lut[seq[i]];
+        rcode[i] = (uint8_t)q;
+        ctab[i] = q < 4 ? (mm4 ^ (x1 << (8 * q))) : mm4;
+    }
 }
 
 __global__ void batch_encode_kernel(const uint8_t *seq, int64_t bytes, const uint8_t *lut, uint8_t *rcode,
@@ -232,9 +336,54 @@ cudaError_t batch_configure() {
                           cudaFuncSetAttribute((const void *)batch_kernel<16, true, WithStores>, A, c),
                           cudaFuncSetAttribute((const void *)batch_kernel<16, false, WithBounds>, A, c),
                           cudaFuncSetAttribute((const void *)batch_kernel<16, true, WithBounds>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_graph_kernel<8, false, NoStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_graph_kernel<8, true, NoStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_graph_kernel<16, false, NoStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_graph_kernel<16, true, NoStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_graph_kernel<16, false, WithStores>, A, c),
+                          cudaFuncSetAttribute((const void *)batch_graph_kernel<16, true, WithStores>, A, c),
                           cudaFuncSetAttribute((const void *)batch_reduce_kernel, A, c),
                           cudaFuncSetAttribute((const void *)batch_encode_kernel, A, c)})
         if (x != cudaSuccess) e = x;
+    return e;
+}
+
+namespace {
+
+template <int R, bool TAB, class S>
+int graph_grid(int sms, int cap) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_graph_kernel<R, TAB, S>, kWarps * 32, 0) != cudaSuccess)
+        nb = 1;
+    int64_t g = (int64_t)std::max(1, nb) * sms;
+    if (cap > 0 && cap < g) g = cap;
+    return (int)std::max<int64_t>(1, g);
+}
+
+template <int R, class S>
+cudaError_t graph_scoring(const GraphHdr *h, int sms, int cap, cudaStream_t st) {
+    batch_graph_kernel<R, true, S><<<graph_grid<R, true, S>(sms, cap), kWarps * 32, 0, st>>>(h);
+    batch_graph_kernel<R, false, S><<<graph_grid<R, false, S>(sms, cap), kWarps * 32, 0, st>>>(h);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t batch_graph_enqueue(const GraphHdr *d_hdr, bool traced, int R, int sms, int max_blocks,
+                                cudaEvent_t ev_mid, cudaStream_t st) {
+    const int wide = 4 * std::max(1, sms);  // grid-stride kernels: 4 blocks of 256 threads per SM
+    graph_prepare_kernel<<<wide, 256, 0, st>>>(d_hdr);
+    graph_decide_kernel<<<1, 256, 0, st>>>(const_cast<GraphHdr *>(d_hdr));
+    graph_encode_kernel<<<wide, 256, 0, st>>>(d_hdr);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (traced) e = graph_scoring<16, WithStores>(d_hdr, sms, max_blocks, st);
+    else if (R == 8) e = graph_scoring<8, NoStores>(d_hdr, sms, max_blocks, st);
+    else e = graph_scoring<16, NoStores>(d_hdr, sms, max_blocks, st);
+    if (e != cudaSuccess) return e;
+    graph_reduce_kernel<<<wide, 256, 0, st>>>(d_hdr);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (ev_mid) e = cudaEventRecordWithFlags(ev_mid, st, cudaEventRecordExternal);
     return e;
 }
 

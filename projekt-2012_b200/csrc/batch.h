@@ -58,6 +58,35 @@ struct BatchArgs {
 constexpr int kBatchR = 16;
 constexpr int kBatchStripRows = 32 * kBatchR;
 
+// One call of a graphed batch.  The captured kernels take only the address of
+// this header, which never moves; the host rewrites the header before every
+// replay, so one graph serves every call with the same grid.
+struct GraphHdr {
+    BatchArgs ba;             // the scoring launch (descriptors, units, work buffers)
+    BestRec *pbest;           // per entry of ba.pairs (slot k)
+    int64_t npairs;           // entries of ba.pairs
+    int64_t seq_bytes;        // bytes at ba.seq
+    int64_t hbuf_entries;     // hand-off entries to reset
+    void *walk_args;          // traced graphs: walker arguments per pair (traceback.cu's layout)
+    int64_t *walk_states;     // traced graphs: walker state per pair
+    uint32_t *walk_dir;       // traced graphs: walker direction scratch (8 CTAs per SM)
+    uint8_t *lut;             // byte -> code (written by the decide kernel)
+    uint32_t *presence;       // 256-bit byte bitmap (all zero between calls)
+    int32_t *out;             // [0..3] the launch's control words, [4] the decided mode
+    uint32_t x1;              // table word: match ^ mismatch byte
+    int32_t tab_ok;           // the scoring values fit the table words
+    int32_t tab;              // 1: at most four distinct byte values (set on the device)
+    int32_t pad_;
+};
+
+// Queues the graphed batch's kernels on st (normally under stream capture):
+// reset and alphabet scan, mode decision, encode, the scoring kernel of either
+// mode (the other one returns at once), the per-pair merge.  With traced = true
+// the scoring kernel keeps every pair's special rows and columns.  ev_mid, if
+// non-null, is recorded (as an external event) after the merge.
+cudaError_t batch_graph_enqueue(const GraphHdr *d_hdr, bool traced, int R, int sms, int max_blocks,
+                                cudaEvent_t ev_mid, cudaStream_t st);
+
 // Launches the batched wavefront over units [0, a.nunits) (a.ctl must be zeroed
 // first), then merges the strips' best cells of pairs [0, npairs) of a.pairs
 // into pbest[slot] (which holds the pair's best so far, or an invalid record).

@@ -146,6 +146,241 @@ void layout_stores(std::vector<BatchPair> &bp, const swb_batch_item *items, cons
     }
 }
 
+
+bool graphs_enabled() {
+    const char *v = std::getenv("SWB_BATCH_GRAPH");
+    return !(v && v[0] == '0');
+}
+
+size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+size_t pow2_at_least(size_t x) {
+    size_t p = 1 << 16;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+// The instantiated graph for a shape (traced or not, rows per lane, grid cap),
+// captured on first use.  Every kernel of it reads the call header at
+// c->g_hdr.p, so the graph never changes for a shape.
+cudaError_t graph_for(swb_ctx *c, bool traced, int R, int cap, cudaGraphExec_t *exec) {
+    for (auto &g : c->graphs)
+        if (g.exec && g.traced == (int)traced && g.R == R && g.cap == cap) {
+            *exec = g.exec;
+            return cudaSuccess;
+        }
+    cudaError_t e;
+    if (!c->cap_stream && (e = cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return e;
+    const GraphHdr *h = (const GraphHdr *)c->g_hdr.p;
+    if ((e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+    cudaError_t q = cudaEventRecordWithFlags(c->ev0, c->cap_stream, cudaEventRecordExternal);
+    if (q == cudaSuccess) q = batch_graph_enqueue(h, traced, R, c->sms, cap, c->ev1, c->cap_stream);
+    if (q == cudaSuccess && traced) q = tb::walk_graph_enqueue(h, c->sms, c->cap_stream);
+    if (q == cudaSuccess && traced) q = cudaEventRecordWithFlags(c->ev2, c->cap_stream, cudaEventRecordExternal);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(c->cap_stream, &graph);
+    if (q != cudaSuccess) e = q;
+    cudaGraphExec_t x = nullptr;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&x, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return e;
+    swb_ctx::GraphEntry *slot = nullptr;
+    for (auto &g : c->graphs)
+        if (!g.exec) {
+            slot = &g;
+            break;
+        }
+    if (!slot) {
+        slot = &c->graphs[c->graph_next];
+        c->graph_next = (c->graph_next + 1) % (int)(sizeof c->graphs / sizeof c->graphs[0]);
+        cudaGraphExecDestroy(slot->exec);
+    }
+    slot->exec = x;
+    slot->traced = traced;
+    slot->R = R;
+    slot->cap = cap;
+    *exec = x;
+    return cudaSuccess;
+}
+
+// Results of a graphed pass, per entry k of bp (pair order[k]).
+struct GraphPass {
+    std::vector<BatchPair> bp;
+    std::vector<BestRec> pbest;
+    bool tab = false;
+    const uint8_t *d_seq = nullptr;
+    const uint8_t *rcode = nullptr;
+    const uint32_t *ctab = nullptr;
+    float ms1 = 0.f, ms2 = 0.f;
+    // traced passes: walker state, reversed ops and crosspoints (pinned host copies)
+    const int64_t *states = nullptr;
+    const char *ops = nullptr;
+    const int64_t *xps = nullptr;
+    std::vector<int64_t> ops_off, xp_off, ops_cap, xp_cap;
+};
+
+// One graphed pass over the active pairs `order` of a host batch: the sequences
+// and every descriptor go to the device in one copy, one graph replay scores
+// every pair (traced: keeping the stores and walking every pair with a positive
+// score), and one copy brings the results back.
+int graph_pass(swb_ctx *c, const uint8_t *h_seq, int64_t seq_bytes, const std::vector<PairInfo> &info,
+               const std::vector<int64_t> &order, const swb_scoring *sc, uint32_t flags, bool traced,
+               swb_batch_result *out, GraphPass &gp) {
+    cudaError_t e;
+    const int R = traced ? kBatchR : batch_score_rows_per_lane();
+    std::vector<int32_t> unit_pair;
+    int64_t hb = 0, srn = 0, scn = 0, ops_total = 0, xp_total = 0;
+    layout_units(info, order, flags, 32 * R, gp.bp, unit_pair, &hb);
+    const int64_t np = (int64_t)gp.bp.size(), nu = (int64_t)unit_pair.size();
+    const int kS = tb::state_slots();
+    if (traced) {
+        layout_stores(gp.bp, out->items, order, &srn, &scn, &ops_total, &xp_total);
+        if ((uint64_t)(srn + scn) * sizeof(int2) > c->opts.hbm_budget_bytes)
+            return ctx_fail(c, SWB_ENOMEM_BUDGET, "traced pairs' special rows and columns exceed the HBM budget");
+        gp.ops_off.resize((size_t)np);
+        gp.xp_off.resize((size_t)np);
+        gp.ops_cap.resize((size_t)np);
+        gp.xp_cap.resize((size_t)np);
+        int64_t oo = 0, xo = 0;
+        for (int64_t k = 0; k < np; ++k) {
+            const BatchPair &d = gp.bp[(size_t)k];
+            gp.ops_off[(size_t)k] = oo;
+            gp.xp_off[(size_t)k] = xo;
+            gp.ops_cap[(size_t)k] = (int64_t)d.m + d.n + 8;
+            gp.xp_cap[(size_t)k] = d.m / out->items[order[(size_t)k]].xpoint_interval + 8;
+            oo += gp.ops_cap[(size_t)k];
+            xo += gp.xp_cap[(size_t)k];
+        }
+        ops_total = oo;
+        xp_total = xo;
+    }
+    // device layouts (16-byte aligned sections)
+    const size_t wa_bytes = tb::walk_args_bytes();
+    const size_t in_pairs = 0, in_units = al16(in_pairs + sizeof(BatchPair) * (size_t)np);
+    const size_t in_walk = al16(in_units + sizeof(int32_t) * (size_t)nu);
+    const size_t in_seq = al16(in_walk + (traced ? wa_bytes * (size_t)np : 0));
+    const size_t in_bytes = al16(in_seq + (size_t)seq_bytes + 64);
+    const size_t w_hbuf = 0, w_gbest = al16(w_hbuf + sizeof(int4) * (size_t)hb);
+    const size_t w_ubest = al16(w_gbest + sizeof(int32_t) * (size_t)np);
+    const size_t w_rcode = al16(w_ubest + sizeof(BestRec) * (size_t)nu);
+    const size_t w_ctab = al16(w_rcode + (size_t)seq_bytes + 64);
+    const size_t w_srows = al16(w_ctab + sizeof(uint32_t) * ((size_t)seq_bytes + 64));
+    const size_t w_scols = al16(w_srows + sizeof(int2) * (size_t)srn);
+    const size_t work_bytes = al16(w_scols + sizeof(int2) * (size_t)scn);
+    const size_t o_ctl = 0, o_pbest = 32;
+    const size_t o_states = al16(o_pbest + sizeof(BestRec) * (size_t)np);
+    const size_t o_xps = al16(o_states + (traced ? sizeof(int64_t) * (size_t)kS * (size_t)np : 0));
+    const size_t o_ops = al16(o_xps + sizeof(int64_t) * 4 * (size_t)xp_total);
+    const size_t out_bytes = al16(o_ops + (size_t)ops_total);
+    const size_t hdr_bytes = al16(sizeof(GraphHdr)), hdr_all = hdr_bytes + 256 + 32;
+    const bool fresh_hdr = c->g_hdr.p == nullptr;
+    if ((e = c->g_hdr.ensure(hdr_all)) != cudaSuccess || (e = c->g_in.ensure(in_bytes)) != cudaSuccess ||
+        (e = c->g_work.ensure(work_bytes)) != cudaSuccess || (e = c->g_out.ensure(out_bytes)) != cudaSuccess ||
+        (traced && (e = c->g_dir.ensure(tb::walk_batch_dir_bytes(c->sms, tb::walk_graph_ctas(c->sms)))) != cudaSuccess) ||
+        (e = c->h_gin.ensure(pow2_at_least(hdr_bytes + in_bytes))) != cudaSuccess ||
+        (e = c->h_gout.ensure(pow2_at_least(out_bytes))) != cudaSuccess)
+        return ctx_cuda_fail(c, e, "graphed batch buffers");
+    uint8_t *dh = (uint8_t *)c->g_hdr.p, *din = (uint8_t *)c->g_in.p, *dw = (uint8_t *)c->g_work.p,
+            *dout = (uint8_t *)c->g_out.p;
+    if (fresh_hdr && (e = cudaMemsetAsync(dh, 0, hdr_all, c->stream)) != cudaSuccess)
+        return ctx_cuda_fail(c, e, "graphed batch header");
+    // the header
+    uint8_t *hs = (uint8_t *)c->h_gin.p;
+    GraphHdr g{};
+    g.ba.open = sc->gap_open;
+    g.ba.ext = sc->gap_extend;
+    g.ba.gx = std::max(sc->gap_open, sc->gap_extend);
+    g.ba.mt1 = sc->match - sc->gap_open;
+    g.ba.mm1 = sc->mismatch - sc->gap_open;
+    const uint32_t mmb = (uint32_t)(uint8_t)(int8_t)g.ba.mm1;
+    g.ba.tab_hi = mmb * 0x01010101u;
+    g.x1 = ((uint32_t)(uint8_t)(int8_t)g.ba.mt1 ^ mmb) & 0xFFu;
+    g.tab_ok = (g.ba.mt1 >= -128 && g.ba.mt1 <= 127 && g.ba.mm1 >= -128 && g.ba.mm1 <= 127) ? 1 : 0;
+    g.ba.seq = din + in_seq;
+    g.ba.cseq = din + in_seq;
+    g.ba.rcode = dw + w_rcode;
+    g.ba.ctab = (const uint32_t *)(dw + w_ctab);
+    g.ba.pairs = (const BatchPair *)(din + in_pairs);
+    g.ba.unit_pair = (const int32_t *)(din + in_units);
+    g.ba.nunits = nu;
+    g.ba.hbuf = (int4 *)(dw + w_hbuf);
+    g.ba.gbest = (int32_t *)(dw + w_gbest);
+    g.ba.ubest = (BestRec *)(dw + w_ubest);
+    g.ba.ctl = (int32_t *)(dout + o_ctl);
+    g.ba.srows = traced ? (int2 *)(dw + w_srows) : nullptr;
+    g.ba.scols = traced ? (int2 *)(dw + w_scols) : nullptr;
+    g.pbest = (BestRec *)(dout + o_pbest);
+    g.npairs = np;
+    g.seq_bytes = seq_bytes;
+    g.hbuf_entries = hb;
+    g.walk_args = traced ? (void *)(din + in_walk) : nullptr;
+    g.walk_states = traced ? (int64_t *)(dout + o_states) : nullptr;
+    g.walk_dir = traced ? (uint32_t *)c->g_dir.p : nullptr;
+    g.lut = dh + hdr_bytes;
+    g.presence = (uint32_t *)(dh + hdr_bytes + 256);
+    g.out = (int32_t *)(dout + o_ctl);
+    std::memcpy(hs, &g, sizeof g);
+    // the inputs
+    uint8_t *hin = hs + hdr_bytes;
+    std::memcpy(hin + in_pairs, gp.bp.data(), sizeof(BatchPair) * (size_t)np);
+    std::memcpy(hin + in_units, unit_pair.data(), sizeof(int32_t) * (size_t)nu);
+    if (traced) {
+        std::vector<tb::WalkInputs> win((size_t)np);
+        for (int64_t k = 0; k < np; ++k) {
+            const BatchPair &d = gp.bp[(size_t)k];
+            tb::WalkInputs &w = win[(size_t)k];
+            std::memset(&w, 0, sizeof w);
+            w.rows = g.ba.seq + d.row_off;
+            w.cols = g.ba.seq + d.col_off;
+            w.m = d.m;
+            w.n = d.n;
+            w.sc = *sc;
+            w.srows = g.ba.srows + d.sr_off;
+            w.scols = g.ba.scols + d.sc_off;
+            w.rr1 = d.m;
+            w.cc1 = d.n;
+            w.xp_interval = out->items[order[(size_t)k]].xpoint_interval;
+            w.ops = (char *)(dout + o_ops) + gp.ops_off[(size_t)k];
+            w.ops_cap = gp.ops_cap[(size_t)k];
+            w.xps = (int64_t *)(dout + o_xps) + 4 * gp.xp_off[(size_t)k];
+            w.xp_cap = gp.xp_cap[(size_t)k];
+        }
+        tb::pack_walk_args(win.data(), np, g.walk_states, hin + in_walk);
+    }
+    if (seq_bytes > 0) std::memcpy(hin + in_seq, h_seq, (size_t)seq_bytes);
+    cudaGraphExec_t exec = nullptr;
+    if ((e = graph_for(c, traced, R, c->max_blocks, &exec)) != cudaSuccess) return ctx_cuda_fail(c, e, "batch graph");
+    uint8_t *hout = (uint8_t *)c->h_gout.p;
+    if ((e = cudaMemcpyAsync(dh, hs, sizeof g, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(din, hin, in_seq + (size_t)seq_bytes, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+        (e = cudaGraphLaunch(exec, c->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(hout, dout, out_bytes, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+        return ctx_cuda_fail(c, e, "batch graph replay");
+    const int32_t *ctl = (const int32_t *)(hout + o_ctl);
+    if (ctl[1] != 0) return ctx_fail(c, SWB_ETIMEOUT, "batch: a bounded wait between strips ran out");
+    gp.tab = ctl[4] != 0;
+    gp.d_seq = g.ba.seq;
+    gp.rcode = g.ba.rcode;
+    gp.ctab = g.ba.ctab;
+    gp.pbest.resize((size_t)np);
+    std::memcpy(gp.pbest.data(), hout + o_pbest, sizeof(BestRec) * (size_t)np);
+    cudaEventElapsedTime(&gp.ms1, c->ev0, c->ev1);
+    if (traced) {
+        cudaEventElapsedTime(&gp.ms2, c->ev1, c->ev2);
+        gp.states = (const int64_t *)(hout + o_states);
+        gp.ops = (const char *)(hout + o_ops);
+        gp.xps = (const int64_t *)(hout + o_xps);
+        for (int64_t k = 0; k < np; ++k) {
+            const int64_t *S = gp.states + (size_t)kS * k;
+            if (S[tb::slot_err()] != 0 || !S[tb::slot_done()])
+                return ctx_fail(c, SWB_ECUDA, "batched walker: inconsistent direction data");
+        }
+    }
+    return SWB_OK;
+}
+
 int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t seq_bytes, const swb_pair_ref *pairs,
               int64_t npairs, const swb_scoring *sc, uint32_t flags, double trace_frac, swb_batch_result *out,
               bool stores_first) {
@@ -190,13 +425,6 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
     cudaError_t e;
-    const uint8_t *d_seq = d_seq_in;
-    if (h_seq) {
-        if ((e = c->b_seq.ensure((size_t)seq_bytes + 64)) != cudaSuccess) return ctx_cuda_fail(c, e, "batch sequences");
-        if ((e = ctx_put(c, c->b_seq.p, h_seq, (size_t)seq_bytes)) != cudaSuccess)
-            return ctx_cuda_fail(c, e, "copy batch sequences");
-        d_seq = (const uint8_t *)c->b_seq.p;
-    }
     // active pairs (both sequences non-empty), longest first (ties: lower index)
     std::vector<int64_t> order;
     order.reserve((size_t)npairs);
@@ -205,6 +433,29 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
     std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
         return info[(size_t)x].m * info[(size_t)x].n > info[(size_t)y].m * info[(size_t)y].n;
     });
+    for (int64_t i = 0; i < npairs; ++i) {
+        int32_t G = 0, T = 0;
+        int64_t P1 = 0, P2 = 0;
+        reference_geometry(info[(size_t)i].m, info[(size_t)i].n, &G, &T, &P1, &P2);
+        out->items[i].xpoint_interval = T > 0 ? 4 * T : 20;
+    }
+    // host batches run as one replayed graph (sequences and descriptors in one
+    // copy, results in one copy); device batches and the store pass of a
+    // partially traced batch launch their kernels directly
+    const bool use_graph = h_seq != nullptr && !order.empty() && graphs_enabled();
+    GraphPass gp;
+    if (use_graph) {
+        int rc = graph_pass(c, h_seq, seq_bytes, info, order, sc, flags, stores_first, out, gp);
+        if (rc != SWB_OK) return rc;
+    }
+
+    const uint8_t *d_seq = d_seq_in;
+    if (h_seq && !use_graph) {
+        if ((e = c->b_seq.ensure((size_t)seq_bytes + 64)) != cudaSuccess) return ctx_cuda_fail(c, e, "batch sequences");
+        if ((e = ctx_put(c, c->b_seq.p, h_seq, (size_t)seq_bytes)) != cudaSuccess)
+            return ctx_cuda_fail(c, e, "copy batch sequences");
+        d_seq = (const uint8_t *)c->b_seq.p;
+    }
 
     BatchArgs base{};
     base.open = sc->gap_open;
@@ -214,7 +465,16 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
     base.mm1 = sc->mismatch - sc->gap_open;
     bool tab = false;
     int32_t launches = 0;
-    if (!order.empty() && base.mt1 >= -128 && base.mt1 <= 127 && base.mm1 >= -128 && base.mm1 <= 127) {
+    if (use_graph) {
+        d_seq = gp.d_seq;
+        tab = gp.tab;
+        if (tab) {
+            base.rcode = gp.rcode;
+            base.ctab = gp.ctab;
+            base.tab_hi = (uint32_t)(uint8_t)(int8_t)base.mm1 * 0x01010101u;
+        }
+        launches += stores_first ? 8 : 6;
+    } else if (!order.empty() && base.mt1 >= -128 && base.mt1 <= 127 && base.mm1 >= -128 && base.mm1 <= 127) {
         // TAB mode when the whole buffer holds at most four distinct bytes
         uint32_t present[256];
         if ((e = c->flags.ensure(256 * sizeof(uint32_t))) != cudaSuccess ||
@@ -239,12 +499,6 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
         }
     }
 
-    for (int64_t i = 0; i < npairs; ++i) {
-        int32_t G = 0, T = 0;
-        int64_t P1 = 0, P2 = 0;
-        reference_geometry(info[(size_t)i].m, info[(size_t)i].n, &G, &T, &P1, &P2);
-        out->items[i].xpoint_interval = T > 0 ? 4 * T : 20;
-    }
     auto ensure_stores = [&](int64_t srn, int64_t scn) -> int {
         if ((uint64_t)(srn + scn) * sizeof(int2) > c->opts.hbm_budget_bytes)
             return ctx_fail(c, SWB_ENOMEM_BUDGET, "traced pairs' special rows and columns exceed the HBM budget");
@@ -262,8 +516,14 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
     float ms1 = 0.f;
     const bool first_stores = stores_first && !order.empty();
     const int R1 = first_stores ? kBatchR : batch_score_rows_per_lane();
-    layout_units(info, order, flags, 32 * R1, bp, unit_pair, &hb);
-    if (!order.empty()) {
+    if (use_graph) {
+        bp = gp.bp;
+        pbest = gp.pbest;
+        ms1 = gp.ms1;
+    } else {
+        layout_units(info, order, flags, 32 * R1, bp, unit_pair, &hb);
+    }
+    if (!order.empty() && !use_graph) {
         BatchArgs a1 = base;
         if (first_stores) {
             layout_stores(bp, out->items, order, &srn, &scn, &ops_total, &xp_total);
@@ -339,98 +599,126 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
             }
         }
         if (!tr.empty()) {
-            ops_total = xp_total = 0;
-            for (size_t k = 0; k < tr.size(); ++k) {
-                ops_total += (int64_t)bpw[k].m + bpw[k].n + 8;
-                xp_total += bpw[k].m / out->items[tr[k]].xpoint_interval + 8;
-            }
             const int kS = tb::state_slots();
-            if ((e = c->b_ops.ensure((size_t)std::max<int64_t>(1, ops_total))) != cudaSuccess ||
-                (e = c->b_xps.ensure(sizeof(int64_t) * 4 * (size_t)std::max<int64_t>(1, xp_total))) != cudaSuccess ||
-                (e = c->b_state.ensure(sizeof(int64_t) * kS * std::max<size_t>(1, tr.size()))) != cudaSuccess ||
-                (e = c->b_walk.ensure(tb::walk_args_bytes() * std::max<size_t>(1, tr.size()))) != cudaSuccess ||
-                (e = c->b_gdir.ensure(tb::walk_batch_dir_bytes(c->sms, (int64_t)tr.size()))) != cudaSuccess)
-                return ctx_cuda_fail(c, e, "batch traceback buffers");
-            std::vector<tb::WalkInputs> win(tr.size());
-            std::vector<int64_t> st((size_t)kS * tr.size(), 0);
-            int64_t oo = 0, xo = 0;
-            std::vector<int64_t> ops_off(tr.size()), xp_off(tr.size());
-            for (size_t k = 0; k < tr.size(); ++k) {
-                const swb_batch_item &it = out->items[tr[k]];
-                const BatchPair &d = bpw[k];
-                tb::WalkInputs &w = win[k];
-                w.rows = d_seq + d.row_off;
-                w.cols = d_seq + d.col_off;
-                w.m = d.m;
-                w.n = d.n;
-                w.sc = *sc;
-                w.score = it.score;
-                w.srows = (const int2 *)c->b_srows.p + d.sr_off;
-                w.scols = (const int2 *)c->b_scols.p + d.sc_off;
-                w.rr0 = 0;
-                w.cc0 = 0;
-                w.rr1 = d.m;
-                w.cc1 = d.n;
-                w.rtop = nullptr;
-                w.rleft = nullptr;
-                w.xp_interval = it.xpoint_interval;
-                w.ops = (char *)c->b_ops.p + oo;
-                w.ops_cap = (int64_t)d.m + d.n + 8;
-                w.xps = (int64_t *)c->b_xps.p + 4 * xo;
-                w.xp_cap = d.m / it.xpoint_interval + 8;
-                ops_off[k] = oo;
-                xp_off[k] = xo;
-                oo += w.ops_cap;
-                xo += w.xp_cap;
-                int64_t *S = st.data() + (size_t)kS * k;
-                S[tb::slot_r()] = it.end_row;
-                S[tb::slot_c()] = it.end_col;
+            // per traced pair: walker state, reversed ops / crosspoints and their capacities
+            std::vector<const int64_t *> tS(tr.size()), tX(tr.size());
+            std::vector<const char *> tO(tr.size());
+            std::vector<int64_t> tOc(tr.size()), tXc(tr.size());
+            std::vector<int64_t> st;
+            std::vector<char> hops;
+            std::vector<int64_t> hxp;
+            if (use_graph && first_stores) {
+                // the graph walked every pair with a positive score already
+                std::vector<int64_t> pos((size_t)npairs, -1);
+                for (size_t k = 0; k < order.size(); ++k) pos[(size_t)order[k]] = (int64_t)k;
+                for (size_t k = 0; k < tr.size(); ++k) {
+                    const size_t q = (size_t)pos[(size_t)tr[k]];
+                    tS[k] = gp.states + (size_t)kS * q;
+                    tO[k] = gp.ops + gp.ops_off[q];
+                    tX[k] = gp.xps + 4 * gp.xp_off[q];
+                    tOc[k] = gp.ops_cap[q];
+                    tXc[k] = gp.xp_cap[q];
+                }
+            } else {
+                ops_total = xp_total = 0;
+                for (size_t k = 0; k < tr.size(); ++k) {
+                    ops_total += (int64_t)bpw[k].m + bpw[k].n + 8;
+                    xp_total += bpw[k].m / out->items[tr[k]].xpoint_interval + 8;
+                }
+                if ((e = c->b_ops.ensure((size_t)std::max<int64_t>(1, ops_total))) != cudaSuccess ||
+                    (e = c->b_xps.ensure(sizeof(int64_t) * 4 * (size_t)std::max<int64_t>(1, xp_total))) != cudaSuccess ||
+                    (e = c->b_state.ensure(sizeof(int64_t) * kS * std::max<size_t>(1, tr.size()))) != cudaSuccess ||
+                    (e = c->b_walk.ensure(tb::walk_args_bytes() * std::max<size_t>(1, tr.size()))) != cudaSuccess ||
+                    (e = c->b_gdir.ensure(tb::walk_batch_dir_bytes(c->sms, (int64_t)tr.size()))) != cudaSuccess)
+                    return ctx_cuda_fail(c, e, "batch traceback buffers");
+                std::vector<tb::WalkInputs> win(tr.size());
+                st.assign((size_t)kS * tr.size(), 0);
+                int64_t oo = 0, xo = 0;
+                std::vector<int64_t> ops_off(tr.size()), xp_off(tr.size());
+                for (size_t k = 0; k < tr.size(); ++k) {
+                    const swb_batch_item &it = out->items[tr[k]];
+                    const BatchPair &d = bpw[k];
+                    tb::WalkInputs &w = win[k];
+                    w.rows = d_seq + d.row_off;
+                    w.cols = d_seq + d.col_off;
+                    w.m = d.m;
+                    w.n = d.n;
+                    w.sc = *sc;
+                    w.score = it.score;
+                    w.srows = (const int2 *)c->b_srows.p + d.sr_off;
+                    w.scols = (const int2 *)c->b_scols.p + d.sc_off;
+                    w.rr0 = 0;
+                    w.cc0 = 0;
+                    w.rr1 = d.m;
+                    w.cc1 = d.n;
+                    w.rtop = nullptr;
+                    w.rleft = nullptr;
+                    w.xp_interval = it.xpoint_interval;
+                    w.ops = (char *)c->b_ops.p + oo;
+                    w.ops_cap = (int64_t)d.m + d.n + 8;
+                    w.xps = (int64_t *)c->b_xps.p + 4 * xo;
+                    w.xp_cap = d.m / it.xpoint_interval + 8;
+                    ops_off[k] = oo;
+                    xp_off[k] = xo;
+                    oo += w.ops_cap;
+                    xo += w.xp_cap;
+                    int64_t *S = st.data() + (size_t)kS * k;
+                    S[tb::slot_r()] = it.end_row;
+                    S[tb::slot_c()] = it.end_col;
+                }
+                std::string err;
+                tb::Scratch scr{};
+                scr.owner = c;
+                scr.get = [](void *owner, void *dst, const void *src, size_t bytes) -> cudaError_t {
+                    return ctx_get((swb_ctx *)owner, dst, src, bytes);
+                };
+                scr.put = [](void *owner, void *dst, const void *src, size_t bytes) -> cudaError_t {
+                    return ctx_put((swb_ctx *)owner, dst, src, bytes);
+                };
+                int rc = tb::walk_batch(c->stream, c->sms, win.data(), (int64_t)win.size(), c->b_walk.p,
+                                        (int64_t *)c->b_state.p, c->b_gdir.p, st.data(), scr, err);
+                if (rc != SWB_OK) return ctx_fail(c, rc, "%s", err.c_str());
+                launches += 1;
+                hops.resize((size_t)std::max<int64_t>(1, oo));
+                hxp.resize((size_t)std::max<int64_t>(4, 4 * xo));
+                if ((e = ctx_get(c, hops.data(), c->b_ops.p, (size_t)oo)) != cudaSuccess ||
+                    (e = ctx_get(c, hxp.data(), c->b_xps.p, sizeof(int64_t) * 4 * (size_t)xo)) != cudaSuccess)
+                    return ctx_cuda_fail(c, e, "batch traceback copy");
+                for (size_t k = 0; k < tr.size(); ++k) {
+                    tS[k] = st.data() + (size_t)kS * k;
+                    tO[k] = hops.data() + ops_off[k];
+                    tX[k] = hxp.data() + 4 * xp_off[k];
+                    tOc[k] = win[k].ops_cap;
+                    tXc[k] = win[k].xp_cap;
+                }
             }
-            std::string err;
-            tb::Scratch scr{};
-            scr.owner = c;
-            scr.get = [](void *owner, void *dst, const void *src, size_t bytes) -> cudaError_t {
-                return ctx_get((swb_ctx *)owner, dst, src, bytes);
-            };
-            scr.put = [](void *owner, void *dst, const void *src, size_t bytes) -> cudaError_t {
-                return ctx_put((swb_ctx *)owner, dst, src, bytes);
-            };
-            int rc = tb::walk_batch(c->stream, c->sms, win.data(), (int64_t)win.size(), c->b_walk.p,
-                                    (int64_t *)c->b_state.p, c->b_gdir.p, st.data(), scr, err);
-            if (rc != SWB_OK) return ctx_fail(c, rc, "%s", err.c_str());
-            launches += 1;
             // gather: ops (end -> start on the device) and crosspoints
             int64_t tot_ops = 0, tot_xp = 0;
             for (size_t k = 0; k < tr.size(); ++k) {
-                const int64_t *S = st.data() + (size_t)kS * k;
-                if (S[tb::slot_nops()] > win[k].ops_cap || S[tb::slot_nxp()] > win[k].xp_cap)
+                const int64_t *S = tS[k];
+                if (S[tb::slot_nops()] > tOc[k] || S[tb::slot_nxp()] > tXc[k])
                     return ctx_fail(c, SWB_ECUDA, "batch traceback output larger than its buffers");
                 tot_ops += S[tb::slot_nops()];
                 tot_xp += S[tb::slot_nxp()] + 2;
             }
-            std::vector<char> hops((size_t)std::max<int64_t>(1, oo));
-            std::vector<int64_t> hxp((size_t)std::max<int64_t>(4, 4 * xo));
-            if ((e = ctx_get(c, hops.data(), c->b_ops.p, (size_t)oo)) != cudaSuccess ||
-                (e = ctx_get(c, hxp.data(), c->b_xps.p, sizeof(int64_t) * 4 * (size_t)xo)) != cudaSuccess)
-                return ctx_cuda_fail(c, e, "batch traceback copy");
             out->ops = (char *)std::malloc((size_t)tot_ops + 1);
             out->xpoints = (swb_xpoint *)std::malloc(sizeof(swb_xpoint) * (size_t)(tot_xp + 2 * ntrace + 1));
             if (!out->ops || !out->xpoints) return ctx_fail(c, SWB_ENOMEM, "out of host memory");
             int64_t po = 0, px = 0;
             for (size_t k = 0; k < tr.size(); ++k) {
                 swb_batch_item &it = out->items[tr[k]];
-                const int64_t *S = st.data() + (size_t)kS * k;
+                const int64_t *S = tS[k];
                 const int64_t nops = S[tb::slot_nops()], nxp = S[tb::slot_nxp()];
                 it.ops_off = po;
                 it.n_ops = nops;
-                std::reverse_copy(hops.data() + ops_off[k], hops.data() + ops_off[k] + nops, out->ops + po);
+                std::reverse_copy(tO[k], tO[k] + nops, out->ops + po);
                 po += nops;
                 it.start_row = S[tb::slot_start_r()];
                 it.start_col = S[tb::slot_start_c()];
                 it.xp_off = px;
                 out->xpoints[px++] = swb_xpoint{0, 0, it.start_row, it.start_col};
                 for (int64_t q = nxp - 1; q >= 0; --q) {
-                    const int64_t *d = hxp.data() + 4 * (xp_off[k] + q);
+                    const int64_t *d = tX[k] + 4 * q;
                     out->xpoints[px++] = swb_xpoint{(int32_t)d[3], (int32_t)d[2], d[0], d[1]};
                 }
                 out->xpoints[px++] = swb_xpoint{0, it.score, it.end_row, it.end_col};
@@ -453,7 +741,8 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
             it.n_xpoints = 1;
             out->xpoints[out->n_xpoints++] = swb_xpoint{0, 0, it.end_row, it.end_col};
         }
-        out->stage2_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
+        out->stage2_ms = (use_graph && first_stores ? (double)gp.ms2 : 0.0) +
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
     }
     out->kernel_launches = launches;
     out->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

@@ -47,6 +47,19 @@ struct swb_ctx {
         b_scols, b_walk, b_ops, b_xps, b_state, b_gdir;
     swb::HostBuf h_stage;  // pinned staging for descriptors and results
     swb::HostBuf h_io;     // pinned staging of ctx_get / ctx_put
+    // graphed batches: the call header (allocated once: the graphs hold its
+    // address), packed inputs, work buffers, packed results, walker scratch, their
+    // pinned staging, and the instantiated graphs by shape
+    swb::DevBuf g_hdr, g_in, g_work, g_out, g_dir;
+    swb::HostBuf h_gin, h_gout;
+    struct GraphEntry {
+        cudaGraphExec_t exec = nullptr;
+        int traced = 0, R = 0, cap = 0;
+    };
+    GraphEntry graphs[4];
+    int graph_next = 0;                  // round-robin replacement when all entries are taken
+    cudaStream_t cap_stream = nullptr;   // private stream the graphs are captured on
+    cudaEvent_t ev2 = nullptr;
     int64_t last_nstrips = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::mutex mu;
@@ -60,7 +73,7 @@ struct swb_ctx {
         for (swb::DevBuf *b : {&rows, &cols, &hbuf, &wbest, &best, &errf, &srows, &scols, &work, &flags, &lut,
                                &rcode, &ctab, &trace, &b_seq, &b_rcode, &b_ctab, &b_pairs, &b_units, &b_hbuf,
                                &b_gbest, &b_ubest, &b_pbest, &b_ctl, &b_srows, &b_scols, &b_walk, &b_ops, &b_xps,
-                               &b_state, &b_gdir})
+                               &b_state, &b_gdir, &g_hdr, &g_in, &g_work, &g_out, &g_dir})
             f(*b);
         for (swb::DevBuf &b : tb) f(b);
     }

@@ -34,6 +34,7 @@
 #include <cstring>
 #include <vector>
 
+#include "batch.h"
 #include "traceback.h"
 
 namespace swb {
@@ -514,7 +515,8 @@ __global__ void __launch_bounds__(32) corridor_walk_kernel(WalkArgs a, const uin
 // Batched pairs: CTA b walks pairs b, b + gridDim.x, ... (each pair's whole
 // matrix is its region), recomputing the blocks on its path on demand into its
 // own region of gdir (kBlockWords words per CTA).
-__global__ void __launch_bounds__(kThreads) walk_batch_kernel(const WalkArgs *args, int64_t n, uint32_t *gdir) {
+// One CTA per pair at a time, pairs p = blockIdx.x, + gridDim.x, ...
+__device__ __forceinline__ void walk_pairs(const WalkArgs *args, int64_t n, uint32_t *gdir) {
     __shared__ Xchg xc;
     __shared__ Stage sg;
     __shared__ int64_t S[kStN];
@@ -532,6 +534,35 @@ __global__ void __launch_bounds__(kThreads) walk_batch_kernel(const WalkArgs *ar
     }
 }
 
+__global__ void __launch_bounds__(kThreads) walk_batch_kernel(const WalkArgs *args, int64_t n, uint32_t *gdir) {
+    walk_pairs(args, n, gdir);
+}
+
+// Graphed batches: every pair's walk starts at the best cell the scoring kernel
+// merged into pbest (a pair without a positive score is marked done at once).
+__global__ void walk_graph_init_kernel(const GraphHdr *h) {
+    const int64_t np = h->npairs;
+    WalkArgs *args = (WalkArgs *)h->walk_args;
+    int64_t *st = h->walk_states;
+    const int32_t open = h->ba.open;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += stride) {
+        const BestRec b = h->pbest[p];
+        const int32_t score = b.valid ? b.ho - open : 0;
+        args[p].score = score;
+        int64_t *S = st + p * kStN;
+#pragma unroll
+        for (int k = 0; k < kStN; ++k) S[k] = 0;
+        S[kStR] = b.row;
+        S[kStC] = b.col;
+        if (score <= 0) S[kStDone] = 1;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) walk_graph_kernel(const GraphHdr *h) {
+    walk_pairs((const WalkArgs *)h->walk_args, h->npairs, h->walk_dir);
+}
+
 }  // namespace
 
 cudaError_t walker_configure() {
@@ -540,7 +571,8 @@ cudaError_t walker_configure() {
     cudaError_t e = cudaSuccess;
     for (cudaError_t x : {cudaFuncSetAttribute((const void *)precompute_kernel, A, c),
                           cudaFuncSetAttribute((const void *)corridor_walk_kernel, A, c),
-                          cudaFuncSetAttribute((const void *)walk_batch_kernel, A, c)})
+                          cudaFuncSetAttribute((const void *)walk_batch_kernel, A, c),
+                          cudaFuncSetAttribute((const void *)walk_graph_kernel, A, c)})
         if (x != cudaSuccess) e = x;
     return e;
 }
@@ -739,6 +771,23 @@ int walk_batch(cudaStream_t st, int sms, const WalkInputs *in, int64_t n, void *
     return SWB_OK;
 }
 
+void pack_walk_args(const WalkInputs *in, int64_t n, int64_t *d_states, void *dst) {
+    WalkArgs *out = (WalkArgs *)dst;
+    for (int64_t i = 0; i < n; ++i) {
+        WalkArgs a = to_args(in[i]);
+        a.st = d_states + i * kStN;
+        std::memcpy(out + i, &a, sizeof a);
+    }
+}
+
+cudaError_t walk_graph_enqueue(const GraphHdr *d_hdr, int sms, cudaStream_t st) {
+    walk_graph_init_kernel<<<std::max(1, sms), 256, 0, st>>>(d_hdr);
+    walk_graph_kernel<<<(unsigned)walk_graph_ctas(sms), kThreads, 0, st>>>(d_hdr);
+    return cudaGetLastError();
+}
+
+int64_t walk_graph_ctas(int sms) { return 8LL * std::max(1, sms); }
+
 size_t walk_args_bytes() { return sizeof(WalkArgs); }
 
 int state_slots() { return kStN; }
@@ -748,6 +797,7 @@ int slot_state() { return kStState; }
 int slot_nops() { return kStNOps; }
 int slot_nxp() { return kStNXp; }
 int slot_done() { return kStDone; }
+int slot_err() { return kStErr; }
 int slot_start_r() { return kStStartR; }
 int slot_start_c() { return kStStartC; }
 int block_rows() { return kBR; }

@@ -6,6 +6,7 @@
 #include "swb_internal.h"
 
 namespace swb {
+struct GraphHdr;
 namespace tb {
 
 // Special-row / special-column spacing of stage 1 for a pair.  Direct mode keeps
@@ -51,6 +52,7 @@ int slot_state();
 int slot_nops();
 int slot_nxp();
 int slot_done();
+int slot_err();
 int slot_start_r();
 int slot_start_c();
 int block_rows();
@@ -83,6 +85,15 @@ int walk_region(cudaStream_t st, int sms, const WalkInputs &in, int64_t *host_st
 int walk_batch(cudaStream_t st, int sms, const WalkInputs *in, int64_t n, void *d_args, int64_t *d_states,
                void *d_dir, int64_t *host_states, const Scratch &scr, std::string &err);
 size_t walk_batch_dir_bytes(int sms, int64_t n);
+
+// Graphed batches (the header's walk_args / walk_states / walk_dir hold every
+// pair of the batch): writes the walker arguments of n pairs into dst (host
+// memory, n * walk_args_bytes() bytes, states at d_states + i * state_slots()),
+// and queues the walker's init and walk kernels, walk_graph_ctas(sms) CTAs whose
+// direction scratch is walk_batch_dir_bytes(sms, walk_graph_ctas(sms)).
+void pack_walk_args(const WalkInputs *in, int64_t n, int64_t *d_states, void *dst);
+cudaError_t walk_graph_enqueue(const GraphHdr *d_hdr, int sms, cudaStream_t st);
+int64_t walk_graph_ctas(int sms);
 
 // Canonical traceback from the end cell in `out` (score, end_row, end_col set by
 // stage 1), using the stage-1 stores laid out by `plan`.  Fills out->ops,

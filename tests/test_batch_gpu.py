@@ -151,3 +151,53 @@ def test_empty_batch_and_bad_ranges(gpu_ctx):
     with pytest.raises(swb200.SwbError) as ei:
         gpu_ctx.batch_align(b"ACGT", np.array([[0, 4, 2, 5]], dtype=np.int64), sc)
     assert ei.value.code == swb200.SWB_EINVAL
+
+
+def _same(r0, r1):
+    for f in ("score", "end_row", "end_col", "start_row", "start_col", "swapped", "traced", "xpoint_interval"):
+        assert (getattr(r0, f) == getattr(r1, f)).all(), f
+    assert r0.ops == r1.ops and r0.xpoints == r1.xpoints and r0.n_traced == r1.n_traced
+
+
+@pytest.mark.parametrize("trace_frac", [0.0, 0.3, 1.0])
+def test_graph_replay_equals_direct_launches(gpu_ctx, monkeypatch, trace_frac):
+    """Host batches run as one replayed CUDA graph; the same batch through the
+    direct launches gives the same results, and replays reuse the captured graph
+    with new sizes in the device header."""
+    rng = random.Random(21)
+    pairs = [_mutated(rng, rng.randint(40, 2600)) for _ in range(150)]
+    pairs += [(b"", b"AC"), (b"A" * 700, b"T" * 600), (b"ACGT" * 300, b"ACGT" * 290)]
+    buf, refs = _pack(pairs)
+    sc = swb200.scoring(2, -3, -5, -2)
+    monkeypatch.setenv("SWB_BATCH_GRAPH", "0")
+    r0 = gpu_ctx.batch_align(buf, refs, sc, 0, trace_frac=trace_frac)
+    monkeypatch.setenv("SWB_BATCH_GRAPH", "1")
+    r1 = gpu_ctx.batch_align(buf, refs, sc, 0, trace_frac=trace_frac)
+    _same(r0, r1)
+    # a smaller batch, then the first one again: same graph, other sizes
+    small = pairs[:7]
+    b2, f2 = _pack(small)
+    r2 = gpu_ctx.batch_align(b2, f2, sc, 0, trace_frac=trace_frac)
+    for i in range(len(small)):
+        assert (r2.score[i], r2.end_row[i], r2.end_col[i]) == (r1.score[i], r1.end_row[i], r1.end_col[i])
+        if trace_frac == 1.0:
+            assert r2.ops[i] == r1.ops[i] and r2.xpoints[i] == r1.xpoints[i]
+    _same(r1, gpu_ctx.batch_align(buf, refs, sc, 0, trace_frac=trace_frac))
+
+
+def test_graph_mode_switch_between_alphabets(gpu_ctx):
+    """The table / compare choice is made on the device each replay: a DNA batch,
+    a batch with more than four byte values, then DNA again."""
+    rng = random.Random(22)
+    sc = (1, -3, -5, -2)
+    dna = [_mutated(rng, rng.randint(100, 900)) for _ in range(30)]
+    prot = [_mutated(rng, rng.randint(100, 900), alph=b"ACDEFGHIKLMNPQRSTVWY") for _ in range(30)]
+    for batch in (dna, prot, dna):
+        buf, refs = _pack(batch)
+        res = gpu_ctx.batch_align(buf, refs, swb200.scoring(*sc), 0, trace_frac=1.0)
+        for i, (a, b) in enumerate(batch):
+            assert (res.score[i], res.end_row[i], res.end_col[i]) == _oracle(a, b, sc, O.TIE_REFERENCE)[:3], i
+            if res.score[i] > 0:
+                rows, cols, _ = O.orient(a, b)
+                assert O.score_ops(rows, cols, O.scoring(*sc), res.start_row[i], res.start_col[i],
+                                   res.ops[i]) == res.score[i]
