@@ -231,8 +231,7 @@ def _convert_batch(r: BatchResult) -> Batch:
     for i in range(n):
         if traced[i]:
             ops.append(allops[ops_off[i]:ops_off[i] + n_ops[i]])
-            xps.append([(r.xpoints[k].row, r.xpoints[k].col, r.xpoints[k].score, r.xpoints[k].gap)
-                        for k in range(xp_off[i], xp_off[i] + n_xp[i])])
+            xps.append(_xpoint_tuples(r.xpoints, int(xp_off[i]), int(n_xp[i])))
         else:
             ops.append("")
             xps.append([])
@@ -251,10 +250,21 @@ def pair_refs(refs) -> "C.Array":
     return arr
 
 
+def _xpoint_tuples(ptr, first: int, count: int) -> list:
+    """(row, col, score, gap) tuples of count XPoint records starting at ptr[first]."""
+    if count <= 0 or not ptr:
+        return []
+    import numpy as np
+    size = C.sizeof(XPoint)
+    raw = C.string_at(C.cast(ptr, C.c_void_p).value + first * size, count * size)
+    a = np.frombuffer(raw, dtype=np.dtype([("gap", np.int32), ("score", np.int32), ("row", np.int64),
+                                           ("col", np.int64)]))
+    return list(zip(a["row"].tolist(), a["col"].tolist(), a["score"].tolist(), a["gap"].tolist()))
+
+
 def _convert(r: Result) -> Alignment:
     ops = C.string_at(r.ops, r.n_ops).decode() if r.n_ops > 0 and r.ops else ""
-    xps = [(r.xpoints[i].row, r.xpoints[i].col, r.xpoints[i].score, r.xpoints[i].gap)
-           for i in range(r.n_xpoints)]
+    xps = _xpoint_tuples(r.xpoints, 0, r.n_xpoints)
     return Alignment(r.score, r.end_row, r.end_col, r.start_row, r.start_col, bool(r.swapped),
                      r.rows, r.cols, r.stage1_ms, r.stage2_ms, r.total_ms, ops, xps,
                      r.xpoint_interval, r.special_interval, r.special_bytes, r.kernel_launches,
