@@ -128,6 +128,17 @@ struct GlobalDir {
     }
 };
 
+// The same layout in shared memory (a block's words copied in from GlobalDir).
+struct SmemDir {
+    const uint32_t *d;
+    __device__ __forceinline__ uint8_t at(int64_t i, int64_t j) const {
+        const int t = (int)(i >> 2), lane = t & 31, warp = t >> 5;
+        const int k = (int)j + lane;
+        return reinterpret_cast<const uint8_t *>(d + (warp * kSteps + k) * 32 + lane)[i & 3];
+    }
+};
+constexpr size_t kDirTileBytes = sizeof(uint32_t) * (size_t)kBlockWords;  // 146,944: a multiple of 16
+
 // Hand-off between the warps of a recompute: warp w publishes (H, F) of its last
 // row (block row 128 (w + 1) - 1) column by column in bnd[w][j] as two 64-bit
 // words {H, gen} and {F, gen}, gen being the recompute's generation; warp w + 1
@@ -484,17 +495,49 @@ __device__ void stage_bytes(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C
 // region (relative to rr0, cc0) is slot map[(bi - bi0) * mw + (bj - bj0)] of
 // gdir, or absent (-1).  Stops where the path enters an absent block, at the
 // start cell or on an error; the state is read from and written back to a.st.
+// Waits (bounded) for phase `parity` of the mbarrier at shared address bar.
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > kXchgWaitCycles) return false;
+    }
+}
+
+// The walk of each block reads the block's direction words from shared memory:
+// on entering a block the warp copies the part the path can still reach (the
+// 128-row chunks at or above the current row, the steps up to the current
+// column + 31) from gdir with one bulk asynchronous copy (cp.async.bulk, the
+// TMA engine) per chunk, completing on an mbarrier, while it stages the
+// block's sequence bytes; every step of the walk is then a shared-memory read
+// instead of a dependent L2 round trip.
 __global__ void __launch_bounds__(32) corridor_walk_kernel(WalkArgs a, const uint32_t *gdir, const int32_t *map,
                                                            int64_t bi0, int64_t bj0, int64_t mh, int64_t mw,
                                                            const int32_t *err) {
+    extern __shared__ __align__(16) uint32_t dtile[];  // kBlockWords words
     __shared__ Stage sg;
     __shared__ int64_t S[kStN];
-    if (threadIdx.x < kStN) S[threadIdx.x] = a.st[threadIdx.x];
+    __shared__ __align__(8) uint64_t bar_mem;
+    const int lane = threadIdx.x;
+    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&bar_mem);
+    if (lane < kStN) S[lane] = a.st[lane];
+    if (lane == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     __syncwarp();
     if (*err) {
-        if (threadIdx.x == 0) S[kStErr] = 1;
+        if (lane == 0) S[kStErr] = 1;
         __syncwarp();
     }
+    uint32_t phase = 0;
+    bool in_flight = false;
     for (;;) {
         const int64_t r = S[kStR], c = S[kStC];
         if (S[kStDone] || S[kStErr] || r < a.rr0 || c < a.cc0) break;
@@ -503,13 +546,40 @@ __global__ void __launch_bounds__(32) corridor_walk_kernel(WalkArgs a, const uin
         const int32_t slot = map[(bi - bi0) * mw + (bj - bj0)];
         if (slot < 0) break;
         const int64_t R0 = a.rr0 + bi * kBR, C0 = a.cc0 + bj * kBC;
+        const int wmax = (int)((r - R0) >> 7);
+        const int kn = (int)(c - C0 + 32 < (int64_t)kSteps ? c - C0 + 32 : (int64_t)kSteps);
+        const uint32_t chunk = (uint32_t)kn * 32u * 4u;
+        __syncwarp();  // the previous block's reads of dtile are done
+        if (lane == 0) {
+            const uint32_t *src = gdir + (int64_t)slot * kBlockWords;
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                         "r"((uint32_t)(wmax + 1) * chunk)
+                         : "memory");
+            for (int w = 0; w <= wmax; ++w)
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        (uint32_t)__cvta_generic_to_shared(dtile + (int64_t)w * kSteps * 32)),
+                    "l"(src + (int64_t)w * kSteps * 32), "r"(chunk), "r"(bar)
+                    : "memory");
+        }
+        in_flight = true;
         stage_bytes(a, R0, r, C0, c, &sg);
+        const bool ok = __all_sync(0xffffffffu, bar_wait(bar, phase & 1));
+        if (!ok) {
+            if (lane == 0) S[kStErr] = 1;
+            __syncwarp();
+            break;
+        }
+        in_flight = false;
+        ++phase;
         __syncwarp();
-        walk(a, R0, C0, GlobalDir{const_cast<uint32_t *>(gdir) + (int64_t)slot * kBlockWords}, &sg, S);
+        walk(a, R0, C0, SmemDir{dtile}, &sg, S);
         __syncwarp();
     }
+    if (in_flight) bar_wait(bar, phase & 1);  // a copy that outlived its wait: let it land (bounded)
     __syncwarp();
-    if (threadIdx.x < kStN) a.st[threadIdx.x] = S[threadIdx.x];
+    if (lane < kStN) a.st[lane] = S[lane];
 }
 
 // Batched pairs: CTA b walks pairs b, b + gridDim.x, ... (each pair's whole
@@ -571,6 +641,8 @@ cudaError_t walker_configure() {
     cudaError_t e = cudaSuccess;
     for (cudaError_t x : {cudaFuncSetAttribute((const void *)precompute_kernel, A, c),
                           cudaFuncSetAttribute((const void *)corridor_walk_kernel, A, c),
+                          cudaFuncSetAttribute((const void *)corridor_walk_kernel,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDirTileBytes),
                           cudaFuncSetAttribute((const void *)walk_batch_kernel, A, c),
                           cudaFuncSetAttribute((const void *)walk_graph_kernel, A, c)})
         if (x != cudaSuccess) e = x;
@@ -718,7 +790,7 @@ int walk_region(cudaStream_t st, int sms, const WalkInputs &in, int64_t *host_st
             return SWB_ECUDA;
         }
         precompute_kernel<<<(unsigned)nblk, kThreads, 0, st>>>(a, d_blk, nblk, gdir, d_err);
-        corridor_walk_kernel<<<1, 32, 0, st>>>(a, gdir, d_map, bi0, bj0, mh, mw, d_err);
+        corridor_walk_kernel<<<1, 32, kDirTileBytes, st>>>(a, gdir, d_map, bi0, bj0, mh, mw, d_err);
         *launches += 2;
         if ((e = cudaGetLastError()) != cudaSuccess ||
             (e = scr.get(scr.owner, host_state, in.dstate, sizeof(int64_t) * kStN)) != cudaSuccess) {
