@@ -189,8 +189,10 @@ void swb_ctx_destroy(swb_ctx *c) {
     c->h_io.release();
     c->h_gin.release();
     c->h_gout.release();
-    for (auto &g : c->graphs)
+    for (auto &g : c->graphs) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+    }
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);

@@ -91,7 +91,8 @@ __device__ __forceinline__ void batch_body(const BatchArgs &g) {
         int32_t u = 0;
         if (lane == 0) u = atomicAdd(&g.ctl[0], 1);
         u = __shfl_sync(0xffffffffu, u, 0);
-        if (u >= g.nunits || ld_volatile(&g.ctl[2]) != 0) break;
+        const int64_t nunits = g.nunits_dev ? *g.nunits_dev : g.nunits;
+        if (u >= nunits || ld_volatile(&g.ctl[2]) != 0) break;
         const BatchPair d = g.pairs[g.unit_pair[u]];
         PairView<S> v;
         v.open = g.open;
@@ -164,13 +165,16 @@ __global__ void __launch_bounds__(kWarps * 32, (std::is_same<S, NoStores>::value
     batch_body<R, TAB, S>(g);
 }
 
-// The graphed form: arguments from the call's header; the instance of the
-// other mode returns at once.
+// The graphed form: the instance of the other mode returns at once.  The
+// arguments stay a kernel parameter, set on the graph when they change (the unit
+// count, which changes every call, is read from the header): read from the
+// header into registers instead, they cost the step loop 5% (306 vs 290 ms on
+// the 100,000-pair batch), because a parameter is a free constant-bank operand
+// and the kernel is at its register cap.
 template <int R, bool TAB, class S>
 __global__ void __launch_bounds__(kWarps * 32, (std::is_same<S, NoStores>::value ? 4 : 3))
-    batch_graph_kernel(const GraphHdr *h) {
+    batch_graph_kernel(BatchArgs g, const GraphHdr *h) {
     if ((h->tab != 0) != TAB) return;
-    const BatchArgs g = h->ba;
     batch_body<R, TAB, S>(g);
 }
 
@@ -244,8 +248,17 @@ __global__ void graph_prepare_kernel(const GraphHdr *h) {
         pbest[i] = z;
     }
     if (h->tab_ok) {
+        // 16 bytes per thread and iteration (the sequence section starts 16-byte aligned)
         const uint8_t *seq = h->ba.seq;
-        for (int64_t i = tid, e = h->seq_bytes; i < e; i += stride) sh[seq[i]] = 1;
+        const int64_t nb = h->seq_bytes, nv = nb >> 4;
+        const uint4 *v = reinterpret_cast<const uint4 *>(seq);
+        for (int64_t i = tid; i < nv; i += stride) {
+            const uint4 w = v[i];
+            const uint32_t q[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+            for (int k = 0; k < 16; ++k) sh[(q[k >> 2] >> (8 * (k & 3))) & 0xFFu] = 1;
+        }
+        for (int64_t i = (nv << 4) + tid; i < nb; i += stride) sh[seq[i]] = 1;
     }
     __syncthreads();
     for (int i = threadIdx.x; i < 256; i += blockDim.x)
@@ -278,15 +291,41 @@ __global__ void graph_decide_kernel(GraphHdr *h) {
 }
 
 // Graph step 3: table encodings of every byte (table path only).
+// 16 bytes per thread and iteration; every section of the graph's buffers starts
+// 16-byte aligned.
 __global__ void graph_encode_kernel(const GraphHdr *h) {
     if (!h->tab) return;
+    __shared__ uint8_t lut[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = h->lut[i];
+    __syncthreads();
     const uint8_t *seq = h->ba.seq;
-    const uint8_t *lut = h->lut;
     uint8_t *rcode = const_cast<uint8_t *>(h->ba.rcode);
     uint32_t *ctab = const_cast<uint32_t *>(h->ba.ctab);
     const uint32_t mm4 = h->ba.tab_hi, x1 = h->x1;
+    const int64_t nb = h->seq_bytes, nv = nb >> 4;
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, e = h->seq_bytes; i < e; i += stride) {
+    for (int64_t i = tid; i < nv; i += stride) {
+        const uint4 w = reinterpret_cast<const uint4 *>(seq)[i];
+        const uint32_t in[4] = {w.x, w.y, w.z, w.w};
+        uint32_t code[4], tw[16];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            uint32_t c = 0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const uint32_t q = lut[(in[k] >> (8 * b)) & 0xFFu];
+                c |= q << (8 * b);
+                tw[4 * k + b] = q < 4 ? (mm4 ^ (x1 << (8 * q))) : mm4;
+            }
+            code[k] = c;
+        }
+        reinterpret_cast<uint4 *>(rcode)[i] = make_uint4(code[0], code[1], code[2], code[3]);
+        uint4 *ct = reinterpret_cast<uint4 *>(ctab) + 4 * i;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) ct[k] = make_uint4(tw[4 * k], tw[4 * k + 1], tw[4 * k + 2], tw[4 * k + 3]);
+    }
+    for (int64_t i = (nv << 4) + tid; i < nb; i += stride) {
         const uint32_t q = lut[seq[i]];
         rcode[i] = (uint8_t)q;
         ctab[i] = q < 4 ? (mm4 ^ (x1 << (8 * q))) : mm4;
@@ -361,30 +400,47 @@ int graph_grid(int sms, int cap) {
 }
 
 template <int R, class S>
-cudaError_t graph_scoring(const GraphHdr *h, int sms, int cap, cudaStream_t st) {
-    batch_graph_kernel<R, true, S><<<graph_grid<R, true, S>(sms, cap), kWarps * 32, 0, st>>>(h);
-    batch_graph_kernel<R, false, S><<<graph_grid<R, false, S>(sms, cap), kWarps * 32, 0, st>>>(h);
+cudaError_t graph_scoring(const GraphHdr *h, int sms, int cap, int64_t max_units, cudaStream_t st) {
+    const BatchArgs placeholder{};  // replaced before the first replay
+    const int64_t need = std::max<int64_t>(1, (max_units + kWarps - 1) / kWarps);
+    const int gt = (int)std::min<int64_t>(graph_grid<R, true, S>(sms, cap), need);
+    const int gc = (int)std::min<int64_t>(graph_grid<R, false, S>(sms, cap), need);
+    batch_graph_kernel<R, true, S><<<gt, kWarps * 32, 0, st>>>(placeholder, h);
+    batch_graph_kernel<R, false, S><<<gc, kWarps * 32, 0, st>>>(placeholder, h);
     return cudaGetLastError();
+}
+
+template <int R, class S>
+void scoring_funcs(const void **f) {
+    f[0] = (const void *)batch_graph_kernel<R, true, S>;
+    f[1] = (const void *)batch_graph_kernel<R, false, S>;
 }
 
 }  // namespace
 
 cudaError_t batch_graph_enqueue(const GraphHdr *d_hdr, bool traced, int R, int sms, int max_blocks,
-                                cudaEvent_t ev_mid, cudaStream_t st) {
-    const int wide = 4 * std::max(1, sms);  // grid-stride kernels: 4 blocks of 256 threads per SM
+                                int64_t max_units, cudaEvent_t ev_mid, cudaStream_t st) {
+    // grid-stride kernels: up to 4 blocks of 256 threads per SM, fewer for small batches
+    const int wide = (int)std::min<int64_t>(4LL * std::max(1, sms), std::max<int64_t>(std::max(1, sms) / 4, max_units / 8));
     graph_prepare_kernel<<<wide, 256, 0, st>>>(d_hdr);
     graph_decide_kernel<<<1, 256, 0, st>>>(const_cast<GraphHdr *>(d_hdr));
     graph_encode_kernel<<<wide, 256, 0, st>>>(d_hdr);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if (traced) e = graph_scoring<16, WithStores>(d_hdr, sms, max_blocks, st);
-    else if (R == 8) e = graph_scoring<8, NoStores>(d_hdr, sms, max_blocks, st);
-    else e = graph_scoring<16, NoStores>(d_hdr, sms, max_blocks, st);
+    if (traced) e = graph_scoring<16, WithStores>(d_hdr, sms, max_blocks, max_units, st);
+    else if (R == 8) e = graph_scoring<8, NoStores>(d_hdr, sms, max_blocks, max_units, st);
+    else e = graph_scoring<16, NoStores>(d_hdr, sms, max_blocks, max_units, st);
     if (e != cudaSuccess) return e;
     graph_reduce_kernel<<<wide, 256, 0, st>>>(d_hdr);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (ev_mid) e = cudaEventRecordWithFlags(ev_mid, st, cudaEventRecordExternal);
     return e;
+}
+
+void batch_graph_scoring_funcs(bool traced, int R, const void **f) {
+    if (traced) scoring_funcs<16, WithStores>(f);
+    else if (R == 8) scoring_funcs<8, NoStores>(f);
+    else scoring_funcs<16, NoStores>(f);
 }
 
 int batch_score_rows_per_lane() {

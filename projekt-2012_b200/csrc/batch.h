@@ -46,6 +46,7 @@ struct BatchArgs {
     const BatchPair *pairs;
     const int32_t *unit_pair;  // work unit -> index into pairs; units are claimed in this order
     int64_t nunits;
+    const int64_t *nunits_dev; // if set, the unit count is read here (graphed launches) instead
     int4 *hbuf;
     int32_t *gbest;            // per pair slot: best H seen so far
     BestRec *ubest;            // per work unit: best cell of that strip
@@ -58,13 +59,16 @@ struct BatchArgs {
 constexpr int kBatchR = 16;
 constexpr int kBatchStripRows = 32 * kBatchR;
 
-// One call of a graphed batch.  The captured kernels take only the address of
-// this header, which never moves; the host rewrites the header before every
-// replay, so one graph serves every call with the same grid.
+// One call of a graphed batch.  The captured kernels take the address of this
+// header, which never moves, and the host rewrites the header before every
+// replay, so one graph serves every call with the same grid; only the two
+// scoring kernels also take the launch's BatchArgs as a parameter, set on the
+// instantiated graph per replay.
 struct GraphHdr {
     BatchArgs ba;             // the scoring launch (descriptors, units, work buffers)
     BestRec *pbest;           // per entry of ba.pairs (slot k)
     int64_t npairs;           // entries of ba.pairs
+    int64_t nunits;           // work units of the scoring launch (ba.nunits_dev points here)
     int64_t seq_bytes;        // bytes at ba.seq
     int64_t hbuf_entries;     // hand-off entries to reset
     void *walk_args;          // traced graphs: walker arguments per pair (traceback.cu's layout)
@@ -82,10 +86,15 @@ struct GraphHdr {
 // Queues the graphed batch's kernels on st (normally under stream capture):
 // reset and alphabet scan, mode decision, encode, the scoring kernel of either
 // mode (the other one returns at once), the per-pair merge.  With traced = true
-// the scoring kernel keeps every pair's special rows and columns.  ev_mid, if
+// the scoring kernel keeps every pair's special rows and columns.  Grids are
+// sized for calls of at most max_units work units (and pairs).  ev_mid, if
 // non-null, is recorded (as an external event) after the merge.
 cudaError_t batch_graph_enqueue(const GraphHdr *d_hdr, bool traced, int R, int sms, int max_blocks,
-                                cudaEvent_t ev_mid, cudaStream_t st);
+                                int64_t max_units, cudaEvent_t ev_mid, cudaStream_t st);
+// The two scoring kernels of such a graph (table path, compare path): their
+// parameters (BatchArgs, header address) are set on the instantiated graph
+// before every replay.
+void batch_graph_scoring_funcs(bool traced, int R, const void **f);
 
 // Launches the batched wavefront over units [0, a.nunits) (a.ctl must be zeroed
 // first), then merges the strips' best cells of pairs [0, npairs) of a.pairs

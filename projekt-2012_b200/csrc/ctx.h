@@ -53,10 +53,15 @@ struct swb_ctx {
     swb::DevBuf g_hdr, g_in, g_work, g_out, g_dir;
     swb::HostBuf h_gin, h_gout;
     struct GraphEntry {
+        cudaGraph_t graph = nullptr;        // kept: its nodes name the exec's nodes
         cudaGraphExec_t exec = nullptr;
-        int traced = 0, R = 0, cap = 0;
+        cudaGraphNode_t scoring[2] = {};     // the scoring kernels (table path, compare path)
+        cudaKernelNodeParams kp[2] = {};     // their launch shapes
+        unsigned char set_args[256] = {};    // the BatchArgs last set on them
+        bool args_valid = false;
+        int traced = 0, R = 0, cap = 0, size_class = 0;
     };
-    GraphEntry graphs[4];
+    GraphEntry graphs[16];
     int graph_next = 0;                  // round-robin replacement when all entries are taken
     cudaStream_t cap_stream = nullptr;   // private stream the graphs are captured on
     cudaEvent_t ev2 = nullptr;

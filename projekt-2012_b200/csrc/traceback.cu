@@ -852,9 +852,10 @@ void pack_walk_args(const WalkInputs *in, int64_t n, int64_t *d_states, void *ds
     }
 }
 
-cudaError_t walk_graph_enqueue(const GraphHdr *d_hdr, int sms, cudaStream_t st) {
-    walk_graph_init_kernel<<<std::max(1, sms), 256, 0, st>>>(d_hdr);
-    walk_graph_kernel<<<(unsigned)walk_graph_ctas(sms), kThreads, 0, st>>>(d_hdr);
+cudaError_t walk_graph_enqueue(const GraphHdr *d_hdr, int sms, int64_t max_pairs, cudaStream_t st) {
+    const int64_t p = std::max<int64_t>(1, max_pairs);
+    walk_graph_init_kernel<<<(unsigned)std::min<int64_t>(std::max(1, sms), (p + 255) / 256), 256, 0, st>>>(d_hdr);
+    walk_graph_kernel<<<(unsigned)std::min<int64_t>(walk_graph_ctas(sms), p), kThreads, 0, st>>>(d_hdr);
     return cudaGetLastError();
 }
 

@@ -89,10 +89,11 @@ size_t walk_batch_dir_bytes(int sms, int64_t n);
 // Graphed batches (the header's walk_args / walk_states / walk_dir hold every
 // pair of the batch): writes the walker arguments of n pairs into dst (host
 // memory, n * walk_args_bytes() bytes, states at d_states + i * state_slots()),
-// and queues the walker's init and walk kernels, walk_graph_ctas(sms) CTAs whose
-// direction scratch is walk_batch_dir_bytes(sms, walk_graph_ctas(sms)).
+// and queues the walker's init and walk kernels for calls of at most max_pairs
+// pairs, up to walk_graph_ctas(sms) CTAs whose direction scratch is
+// walk_batch_dir_bytes(sms, walk_graph_ctas(sms)).
 void pack_walk_args(const WalkInputs *in, int64_t n, int64_t *d_states, void *dst);
-cudaError_t walk_graph_enqueue(const GraphHdr *d_hdr, int sms, cudaStream_t st);
+cudaError_t walk_graph_enqueue(const GraphHdr *d_hdr, int sms, int64_t max_pairs, cudaStream_t st);
 int64_t walk_graph_ctas(int sms);
 
 // Canonical traceback from the end cell in `out` (score, end_row, end_col set by

@@ -227,14 +227,13 @@ def _convert_batch(r: BatchResult) -> Batch:
     ops_off, n_ops = col("ops_off", np.int64), col("n_ops", np.int64)
     xp_off, n_xp = col("xp_off", np.int64), col("n_xpoints", np.int64)
     allops = C.string_at(r.ops, r.ops_bytes).decode() if r.ops and r.ops_bytes > 0 else ""
-    ops, xps = [], []
-    for i in range(n):
-        if traced[i]:
-            ops.append(allops[ops_off[i]:ops_off[i] + n_ops[i]])
-            xps.append(_xpoint_tuples(r.xpoints, int(xp_off[i]), int(n_xp[i])))
-        else:
-            ops.append("")
-            xps.append([])
+    allxp = _xpoint_tuples(r.xpoints, 0, r.n_xpoints)
+    ops = [""] * n
+    xps = [[] for _ in range(n)]
+    for i in np.flatnonzero(traced).tolist():
+        o, x = int(ops_off[i]), int(xp_off[i])
+        ops[i] = allops[o:o + int(n_ops[i])]
+        xps[i] = allxp[x:x + int(n_xp[i])]
     return Batch(score, col("end_row", np.int64), col("end_col", np.int64), col("start_row", np.int64),
                  col("start_col", np.int64), swapped.astype(bool), traced.astype(bool), ops, xps, xpi,
                  r.n_traced, r.cells, r.stage1_ms, r.stage2_ms, r.total_ms, r.kernel_launches)
