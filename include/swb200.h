@@ -286,6 +286,30 @@ void swb_server_destroy(swb_server *s);
  * out[3*strips] (cap entries available); *count receives the strip count. */
 int swb_trace_copy(swb_ctx *ctx, int64_t *out, int64_t cap, int64_t *count);
 
+/* ------------------------------------------------------------ gap lists
+ * The alignment of a result as the gap lists the reference's renderer reads
+ * (visualOutput, src/Visualisation.cpp:11-127; it was never called there): per
+ * sequence, records {begin, length} meaning `length` gap characters stand
+ * before the base at 0-based index `begin` of that sequence.  "first" is the
+ * rows sequence of the result (the longer one, A unless swapped), "second" the
+ * columns sequence.  Runs of 'I' open gaps in the first sequence, runs of 'D'
+ * in the second. */
+typedef struct swb_gap {
+    int32_t begin;
+    int32_t length;
+} swb_gap;
+
+/* Writes up to *_cap records to first / second (either may be NULL with cap 0)
+ * and the full record counts to *n_first / *n_second.  SWB_EINVAL when result
+ * or a count pointer is NULL, when the operation string is malformed, or when a
+ * buffer is too small (the counts are still written). */
+int swb_gap_lists(const swb_result *result, swb_gap *first, int64_t first_cap, int64_t *n_first,
+                  swb_gap *second, int64_t second_cap, int64_t *n_second);
+
+/* The same lists as the reference's binary gap-list files: consecutive native
+ * int32 pairs (begin, length), the layout visualOutput reads with fread. */
+int swb_gap_lists_write(const swb_result *result, const char *first_path, const char *second_path);
+
 /* Library version string. */
 const char *swb_version(void);
 

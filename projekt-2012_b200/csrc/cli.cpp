@@ -11,7 +11,8 @@
 //   "\t>Alignment score: %d at [%d, %d]\n\n"  1-based end     (main.cu:224)
 //   "Found %d crosspoints:\n" "\t>xPoint[%d]: [%d, %d] = %d\n" (main.cu:245-248)
 // followed by the alignment in the 3-line, 50-column blocks of the reference's
-// (never called) visualOutput (src/Visualisation.cpp:62-127).
+// (never called) visualOutput (src/Visualisation.cpp:62-127); with SWB_GAP_LISTS
+// set, also the gap-list files that renderer reads (:11-43).
 // Other lines are informational, as in the reference.
 #include <chrono>
 #include <cstdio>
@@ -123,6 +124,13 @@ int main(int argc, char *argv[]) {
             const unsigned char *rows = res.swapped ? B.seq.data() : A.seq.data();
             const unsigned char *cols = res.swapped ? A.seq.data() : B.seq.data();
             render_alignment(res, rows, cols);
+            // the reference renderer's binary gap lists, when asked for (SWB_GAP_LISTS=<prefix>
+            // writes <prefix>.first.bin and <prefix>.second.bin)
+            if (const char *g = std::getenv("SWB_GAP_LISTS")) {
+                const std::string p(g);
+                if (swb_gap_lists_write(&res, (p + ".first.bin").c_str(), (p + ".second.bin").c_str()) != SWB_OK)
+                    std::printf("Gap lists not written: %s\n", swb_last_error(nullptr));
+            }
         }
     }
     swb_result_free(&res);

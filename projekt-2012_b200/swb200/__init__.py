@@ -160,6 +160,11 @@ def lib():
         L.swb_probe_cell_peak.restype = C.c_int
         L.swb_probe_latency.argtypes = [C.c_int32, C.POINTER(C.c_double), C.c_int32]
         L.swb_probe_latency.restype = C.c_int
+        L.swb_gap_lists.argtypes = [C.POINTER(Result), C.c_void_p, C.c_int64, C.POINTER(C.c_int64), C.c_void_p,
+                                    C.c_int64, C.POINTER(C.c_int64)]
+        L.swb_gap_lists.restype = C.c_int
+        L.swb_gap_lists_write.argtypes = [C.POINTER(Result), C.c_char_p, C.c_char_p]
+        L.swb_gap_lists_write.restype = C.c_int
         _lib = L
     return _lib
 
@@ -268,6 +273,52 @@ def _convert(r: Result) -> Alignment:
                      r.rows, r.cols, r.stage1_ms, r.stage2_ms, r.total_ms, ops, xps,
                      r.xpoint_interval, r.special_interval, r.special_bytes, r.kernel_launches,
                      r.n_ops)
+
+
+class Gap(C.Structure):
+    _fields_ = [("begin", C.c_int32), ("length", C.c_int32)]
+
+
+def _result_view(ops: str, start_row: int, start_col: int):
+    """A Result carrying an operation string (kept alive by the returned buffer)."""
+    raw = ops.encode()
+    buf = C.create_string_buffer(raw, len(raw) + 1)
+    r = Result()
+    r.ops = C.cast(buf, C.c_void_p)
+    r.n_ops = len(raw)
+    r.start_row = start_row
+    r.start_col = start_col
+    return r, buf
+
+
+def gap_lists(al) -> Tuple[List[Tuple[int, int]], List[Tuple[int, int]]]:
+    """The alignment's gap lists in the reference renderer's format
+    (src/Visualisation.cpp:11-127): for the first (rows) and second (columns)
+    sequence, (begin, length) = `length` gaps before the base at index `begin`.
+    `al` needs ops, start_row and start_col (an Alignment)."""
+    r, keep = _result_view(al.ops, al.start_row, al.start_col)
+    n1, n2 = C.c_int64(), C.c_int64()
+    rc = lib().swb_gap_lists(C.byref(r), None, 0, C.byref(n1), None, 0, C.byref(n2))
+    if rc != SWB_OK and (n1.value == 0 and n2.value == 0):
+        raise SwbError(rc, lib().swb_last_error(None).decode())
+    a, b = (Gap * max(1, n1.value))(), (Gap * max(1, n2.value))()
+    rc = lib().swb_gap_lists(C.byref(r), C.cast(a, C.c_void_p), n1.value, C.byref(n1), C.cast(b, C.c_void_p),
+                             n2.value, C.byref(n2))
+    if rc != SWB_OK:
+        raise SwbError(rc, lib().swb_last_error(None).decode())
+    del keep
+    return ([(a[i].begin, a[i].length) for i in range(n1.value)],
+            [(b[i].begin, b[i].length) for i in range(n2.value)])
+
+
+def write_gap_lists(al, first_path: str, second_path: str) -> None:
+    """Writes the two gap lists as the reference's binary files (int32 begin,
+    int32 length records)."""
+    r, keep = _result_view(al.ops, al.start_row, al.start_col)
+    rc = lib().swb_gap_lists_write(C.byref(r), first_path.encode(), second_path.encode())
+    del keep
+    if rc != SWB_OK:
+        raise SwbError(rc, lib().swb_last_error(None).decode())
 
 
 class Context:
