@@ -310,6 +310,31 @@ int swb_gap_lists(const swb_result *result, swb_gap *first, int64_t first_cap, i
  * int32 pairs (begin, length), the layout visualOutput reads with fread. */
 int swb_gap_lists_write(const swb_result *result, const char *first_path, const char *second_path);
 
+/* ---------------------------------------------------------------- FASTA
+ * Reads a FASTA file.  flags = 0: the reference loader's rules exactly
+ * (FASTAsequence::load, src/FASTA.cpp:39-86): one record; the first byte must be
+ * '>'; the name is the first line without '>' and its last character (at most
+ * 199 bytes read); the first 299 bytes of that line are skipped; every other
+ * byte except '
+' and '' is sequence, unchanged.  With SWB_FASTA_MULTI every
+ * line starting with '>' opens a record whose name is that whole line (any
+ * length, without '>' and the line end), lines starting with ';' are comments,
+ * and blanks, tabs and line ends are dropped from sequences.  SWB_FASTA_UPPER
+ * folds a-z to A-Z in sequences (the kernels compare bytes as they are).
+ * *records receives `*count` records owned by the caller (swb_fasta_free).
+ * SWB_EINVAL for a missing file or one that does not start with '>'. */
+#define SWB_FASTA_MULTI 0x1u
+#define SWB_FASTA_UPPER 0x2u
+
+typedef struct swb_fasta_record {
+    char *name;     /* NUL-terminated */
+    uint8_t *seq;
+    int64_t len;
+} swb_fasta_record;
+
+int swb_fasta_load(const char *path, uint32_t flags, swb_fasta_record **records, int64_t *count);
+void swb_fasta_free(swb_fasta_record *records, int64_t count);
+
 /* Library version string. */
 const char *swb_version(void);
 

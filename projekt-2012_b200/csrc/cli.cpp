@@ -20,8 +20,19 @@
 #include <cstring>
 #include <string>
 
-#include "fasta.h"
 #include "swb200.h"
+
+// A loaded sequence (a view of a swb_fasta_record).
+struct Seq {
+    std::string name;
+    struct Bytes {
+        const unsigned char *p;
+        size_t n;
+        const unsigned char *data() const { return p; }
+        size_t size() const { return n; }
+    } seq;
+    Seq(const char *nm, const unsigned char *p, size_t n) : name(nm), seq{p, n} {}
+};
 
 static void exit_with_msg(const char *msg, int code) {
     std::printf("ERROR\n");
@@ -64,10 +75,13 @@ int main(int argc, char *argv[]) {
         std::printf("Expected 6 input arguments, not %d!\n\n", argc - 1);
         return -1;
     }
-    swb::FastaRecord A, B;
+    // the reference loader's rules (flags 0): one record, bytes kept as they are
+    swb_fasta_record *fa = nullptr, *fb = nullptr;
+    int64_t na = 0, nb = 0;
     std::printf("> Loading input sequences... ");
-    if (!swb::fasta_load(argv[1], &A) || !swb::fasta_load(argv[2], &B))
+    if (swb_fasta_load(argv[1], 0, &fa, &na) != SWB_OK || swb_fasta_load(argv[2], 0, &fb, &nb) != SWB_OK)
         exit_with_msg("An error has occured while loading input sequences.", -1);
+    const Seq A{fa[0].name, fa[0].seq, (size_t)fa[0].len}, B{fb[0].name, fb[0].seq, (size_t)fb[0].len};
     std::printf("DONE\n\n");
     std::printf("First sequence of length %d:\n%s\n\n", (int)A.seq.size(), A.name.c_str());
     std::printf("Second sequence of length %d:\n%s\n\n", (int)B.seq.size(), B.name.c_str());
@@ -135,5 +149,7 @@ int main(int argc, char *argv[]) {
     }
     swb_result_free(&res);
     swb_ctx_destroy(ctx);
+    swb_fasta_free(fa, na);
+    swb_fasta_free(fb, nb);
     return 0;
 }

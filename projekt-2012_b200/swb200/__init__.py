@@ -165,6 +165,11 @@ def lib():
         L.swb_gap_lists.restype = C.c_int
         L.swb_gap_lists_write.argtypes = [C.POINTER(Result), C.c_char_p, C.c_char_p]
         L.swb_gap_lists_write.restype = C.c_int
+        L.swb_fasta_load.argtypes = [C.c_char_p, C.c_uint32, C.POINTER(C.POINTER(FastaRecord)),
+                                     C.POINTER(C.c_int64)]
+        L.swb_fasta_load.restype = C.c_int
+        L.swb_fasta_free.argtypes = [C.POINTER(FastaRecord), C.c_int64]
+        L.swb_fasta_free.restype = None
         _lib = L
     return _lib
 
@@ -273,6 +278,29 @@ def _convert(r: Result) -> Alignment:
                      r.rows, r.cols, r.stage1_ms, r.stage2_ms, r.total_ms, ops, xps,
                      r.xpoint_interval, r.special_interval, r.special_bytes, r.kernel_launches,
                      r.n_ops)
+
+
+FASTA_MULTI = 0x1
+FASTA_UPPER = 0x2
+
+
+class FastaRecord(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("seq", C.c_void_p), ("len", C.c_int64)]
+
+
+def fasta_load(path: str, flags: int = 0) -> List[Tuple[str, bytes]]:
+    """Records (name, sequence bytes) of a FASTA file: flags 0 = the reference
+    loader's single-record rules (src/FASTA.cpp:39-86); FASTA_MULTI = every '>'
+    line opens a record; FASTA_UPPER folds lower case."""
+    recs, n = C.POINTER(FastaRecord)(), C.c_int64()
+    rc = lib().swb_fasta_load(path.encode(), flags, C.byref(recs), C.byref(n))
+    if rc != SWB_OK:
+        raise SwbError(rc, lib().swb_last_error(None).decode())
+    try:
+        return [(recs[i].name.decode(errors="replace"), C.string_at(recs[i].seq, recs[i].len))
+                for i in range(n.value)]
+    finally:
+        lib().swb_fasta_free(recs, n.value)
 
 
 class Gap(C.Structure):
