@@ -145,6 +145,19 @@ def profile_traffic(workload_name):
     return None
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (from /proc/cpuinfo) and logical CPU count."""
+    name = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                name = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return f"{name}, {os.cpu_count()} logical CPUs"
+
+
 def cpu_baseline(a: bytes, b: bytes, sc):
     """The oracle's multithreaded CPU wavefront (same int32 recurrence) on a
     bounded sample of the same pair: a band of rows against all columns, sized
@@ -160,7 +173,7 @@ def cpu_baseline(a: bytes, b: bytes, sc):
     nrows = max(1, min(len(rows) - lo, int(rate * 12.0 // len(cols))))
     _, t = O.stage1_mt(rows[lo:lo + nrows], cols, O.scoring(*sc), threads=threads)
     cells = nrows * len(cols)
-    return {"value": cells / t / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port",
+    return {"value": cells / t / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port", "cpu": cpu_model(),
             "sample": f"rows {lo}..{lo + nrows} of the rows sequence x all {len(cols)} columns "
                       f"({cells:.3e} cells, {t:.1f} s), score + end cell"}
 
@@ -202,7 +215,7 @@ def reference_arm(args):
             "impl": "reference",
             "config": {"workload": desc, "sample_rows": len(sa), "sample_cols": len(sb),
                        "stages": "stage 1 (score + end cell)"},
-            "cpu_baseline": {"value": v, "unit": "GCUPS", "cores": cores, "kind": "reference",
+            "cpu_baseline": {"value": v, "unit": "GCUPS", "cores": cores, "kind": "reference", "cpu": cpu_model(),
                              "sample": f"{len(sa)} x {len(sb)} sub-pair of the workload, stage 1, "
                                        f"reference kernels on host threads"},
             "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
