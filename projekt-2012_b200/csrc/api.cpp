@@ -320,12 +320,19 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     a.tie.T = T;
     a.tie.C = refok ? P2 / G : 1;
 
-    // rows per lane: an override, else the autotuner (strips must tile the
-    // special-row spacing when special rows are kept)
-    const bool stores = sr_interval_rows > 0 || sc_interval > 0;
+    // rows per lane: an override, else the autotuner.  Strips must tile the
+    // special-row spacing when special rows are kept; sr_interval_rows < 0 asks
+    // for a special row at every strip bottom with the strip height left to the
+    // tuner (448 or 512 rows: the walker's block grid follows it).
+    const bool strip_rows = sr_interval_rows < 0;
+    const bool stores = sr_interval_rows != 0 || sc_interval > 0;
     int R = 16;
-    if (const char *rv = std::getenv("SWB_STAGE1_R")) R = std::atoi(rv);  // override: 8, 16 or 32
-    else R = autotune_rows_per_lane(c, a, tab, stores, 16);
+    if (const char *rv = std::getenv("SWB_STAGE1_R")) R = std::atoi(rv);  // override: 8, 14, 16 or 32
+    else R = autotune_rows_per_lane(c, a, tab, stores, 16, strip_rows);
+    if (strip_rows) {
+        if (R != 14 && R != 16) R = 16;
+        sr_interval_rows = 32LL * R;
+    }
     if (sr_interval_rows > 0 && (R > 16 || sr_interval_rows % (32 * R) != 0)) R = 16;
     Stage1Plan plan = stage1_plan(m, n, c->sms, R, tab);
     if (c->max_blocks > 0 && plan.blocks > c->max_blocks) plan.blocks = c->max_blocks;
@@ -423,6 +430,9 @@ int align_device(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_
         plan = tb::plan_for(c->opts, m, n);
         sr_interval = plan.kr;
         sc_interval = plan.kc;
+        // direct mode, with room for special rows every 448 rows as well: the
+        // strip height (448 or 512) is tuned and the walker's grid follows it
+        if (!plan.level1 && !tb::plan_for(c->opts, m, n, 448).level1) sr_interval = -1;
     } else if (c->opts.special_interval > 0 && !(flags & SWB_FLAG_NO_SPECIAL)) {
         sr_interval = c->opts.special_interval;  // inspection of special rows only
     }
@@ -434,6 +444,7 @@ int align_device(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_
     out->stage1_ms = ms;
     out->kernel_launches += c->last_launches;
     out->special_interval = (int32_t)c->last_sr_interval;
+    if (!score_only && sr_interval < 0) plan = tb::plan_for(c->opts, m, n, c->last_sr_interval);
     out->special_bytes = (int64_t)sizeof(int2) * nsr * n + (sc_interval > 0 ? (int64_t)sizeof(int2) * (n / sc_interval) * m : 0);
     if (best.valid) {
         out->score = best.ho - sc->gap_open;

@@ -54,7 +54,7 @@ void load_locked() {
     while (std::fgets(line, sizeof line, f)) {
         char a[32], b[16], c[16], d[16], e[16];
         int R = 0;
-        if (std::sscanf(line, "%31s %15s %15s %15s %15s %d", a, b, c, d, e, &R) == 6 && (R == 8 || R == 16 || R == 32))
+        if (std::sscanf(line, "%31s %15s %15s %15s %15s %d", a, b, c, d, e, &R) == 6 && (R == 8 || R == 14 || R == 16 || R == 32))
             g_table[std::string(a) + " " + b + " " + c + " " + d + " " + e] = R;
     }
     std::fclose(f);
@@ -72,18 +72,22 @@ void store_locked(const std::string &key, int R) {
 
 }  // namespace
 
-int autotune_rows_per_lane(swb_ctx *c, const Stage1Args &base, bool tab, bool stores, int fallback) {
+int autotune_rows_per_lane(swb_ctx *c, const Stage1Args &base, bool tab, bool stores, int fallback,
+                           bool strip_rows) {
     // pairs below this many cells are not worth a probe
     constexpr double kMinCells = 2e10;
     if ((double)base.m * (double)base.n < kMinCells) return fallback;
-    const std::string key = key_of(c->sms, stores, tab, base.m, base.n);
+    const std::string key = key_of(c->sms, stores, tab, base.m, base.n) + (strip_rows ? "|strip" : "");
     {
         std::lock_guard<std::mutex> lk(g_mu);
         load_locked();
         auto it = g_table.find(key);
         if (it != g_table.end()) return it->second;
     }
-    std::vector<int> cands = stores ? std::vector<int>{8, 16} : std::vector<int>{8, 16, 32};
+    // score only: any height; stores at fixed intervals (level 1): heights that
+    // divide them; stores at every strip bottom (direct traceback): 448 or 512 rows
+    std::vector<int> cands = !stores ? std::vector<int>{8, 14, 16, 32}
+                                     : (strip_rows ? std::vector<int>{14, 16} : std::vector<int>{8, 16});
     const int64_t np = std::min<int64_t>(base.n, 1 << 18);
     int bestR = fallback;
     float bestMs = 1e30f;

@@ -105,6 +105,8 @@ cudaError_t ctx_put(swb_ctx *c, void *dev_dst, const void *src, size_t bytes);
 // the pair's shape bucket, else timed probes of every candidate on a slice of the
 // pair described by `base` (rows, columns, encodings, scoring and the hand-off,
 // best and error buffers must be set).  Small pairs get `fallback`.
-int autotune_rows_per_lane(swb_ctx *c, const Stage1Args &base, bool tab, bool stores, int fallback);
+// strip_rows: special rows at every strip bottom, height 448 or 512 rows.
+int autotune_rows_per_lane(swb_ctx *c, const Stage1Args &base, bool tab, bool stores, int fallback,
+                           bool strip_rows = false);
 
 }  // namespace swb

@@ -192,6 +192,10 @@ cudaError_t stage1_configure() {
     cudaError_t e = cudaSuccess;
     for (cudaError_t x : {cudaFuncSetAttribute((const void *)stage1_kernel<8, false, false>, A, c),
                           cudaFuncSetAttribute((const void *)stage1_kernel<8, true, false>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<14, false, false>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<14, true, false>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<14, false, true>, A, c),
+                          cudaFuncSetAttribute((const void *)stage1_kernel<14, true, true>, A, c),
                           cudaFuncSetAttribute((const void *)stage1_kernel<16, false, false>, A, c),
                           cudaFuncSetAttribute((const void *)stage1_kernel<16, true, false>, A, c),
                           cudaFuncSetAttribute((const void *)stage1_kernel<32, false, false>, A, c),
@@ -212,6 +216,7 @@ cudaError_t stage1_configure() {
 int stage1_max_blocks_per_sm(int R, bool tab) {
     switch (R) {
         case 8: return tab ? max_blocks_r<8, true>() : max_blocks_r<8, false>();
+        case 14: return tab ? max_blocks_r<14, true>() : max_blocks_r<14, false>();
         case 16: return tab ? max_blocks_r<16, true>() : max_blocks_r<16, false>();
         case 32: return tab ? max_blocks_r<32, true>() : max_blocks_r<32, false>();
         default: return 0;
@@ -220,7 +225,7 @@ int stage1_max_blocks_per_sm(int R, bool tab) {
 
 Stage1Plan stage1_plan(int64_t m, int64_t n, int device_sms, int R_hint, bool tab) {
     Stage1Plan p;
-    p.R = (R_hint == 8 || R_hint == 16 || R_hint == 32) ? R_hint : 16;
+    p.R = (R_hint == 8 || R_hint == 14 || R_hint == 16 || R_hint == 32) ? R_hint : 16;
     p.tab = tab;
     p.warps_per_block = kWarps;
     p.strip_rows = 32LL * p.R;
@@ -242,6 +247,7 @@ cudaError_t stage1_launch(Stage1Args &a, const Stage1Plan &p, cudaStream_t st) {
     if (p.tab) {
         switch (p.R) {
             case 8: return launch_r<8, true>(a, p, st);
+            case 14: return launch_r<14, true>(a, p, st);
             case 16: return launch_r<16, true>(a, p, st);
             case 32: return launch_r<32, true>(a, p, st);
             default: return cudaErrorInvalidValue;
@@ -249,6 +255,7 @@ cudaError_t stage1_launch(Stage1Args &a, const Stage1Plan &p, cudaStream_t st) {
     }
     switch (p.R) {
         case 8: return launch_r<8, false>(a, p, st);
+        case 14: return launch_r<14, false>(a, p, st);
         case 16: return launch_r<16, false>(a, p, st);
         case 32: return launch_r<32, false>(a, p, st);
         default: return cudaErrorInvalidValue;

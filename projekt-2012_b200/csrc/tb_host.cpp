@@ -62,6 +62,7 @@ int traceback(cudaStream_t st, int sms, const uint8_t *d_rows, int64_t m, const 
     w.dstate = d_state;
     int rc;
     if (!plan.level1) {
+        w.br = plan.br;
         w.srows = d_srows;
         w.scols = d_scols;
         w.rr0 = 0;

@@ -68,6 +68,7 @@ struct WalkArgs {
     int64_t *xps;                  // reversed crosspoints: 4 int64 each (row, col, score, gap)
     int64_t xp_cap;
     int64_t *st;                   // walker state in/out: see kSt* below
+    int32_t br;                    // block rows of the region's grid (the special-row spacing), <= kBR
 };
 
 // walker state slots
@@ -81,7 +82,7 @@ __device__ __forceinline__ int2 top_hf(const WalkArgs &a, int64_t R0, int64_t c)
         if (c < a.cc0) return make_int2((a.rtop && a.rleft) ? a.rtop[-1].x : 0, 0);  // the corner
         return a.rtop ? a.rtop[c - a.cc0] : make_int2(0, 0);
     }
-    const int64_t q = (R0 - a.rr0) / kBR - 1;
+    const int64_t q = (R0 - a.rr0) / a.br - 1;
     if (c < a.cc0) return make_int2(a.rleft ? a.rleft[R0 - 1 - a.rr0].x : 0, 0);
     return a.srows[q * (a.cc1 - a.cc0) + (c - a.cc0)];
 }
@@ -444,7 +445,7 @@ __device__ void walk_body(const WalkArgs &a, const D &dir, Xchg *xc, Stage *sg, 
     for (; guard < (1 << 30); ++guard) {
         const int64_t r = S[kStR], c = S[kStC];
         if (S[kStDone] || S[kStErr] || r < a.rr0 || c < a.cc0) break;
-        const int64_t R0 = a.rr0 + ((r - a.rr0) / kBR) * kBR;
+        const int64_t R0 = a.rr0 + ((r - a.rr0) / a.br) * a.br;
         const int64_t C0 = a.cc0 + ((c - a.cc0) / kBC) * kBC;
         stage_block(a, R0, r, C0, c, sg);
         __syncthreads();
@@ -475,7 +476,7 @@ __global__ void __launch_bounds__(kThreads) precompute_kernel(WalkArgs a, const 
     uint32_t gen = 0;
     for (int64_t b = blockIdx.x; b < nblk; b += gridDim.x) {
         const int64_t R0 = blk[2 * b], C0 = blk[2 * b + 1];
-        const int64_t R1 = min(R0 + kBR - 1, a.rr1 - 1), C1 = min(C0 + kBC - 1, a.cc1 - 1);
+        const int64_t R1 = min(R0 + a.br - 1, a.rr1 - 1), C1 = min(C0 + kBC - 1, a.cc1 - 1);
         __syncthreads();
         stage_block(a, R0, R1, C0, C1, &sg);
         __syncthreads();
@@ -541,11 +542,11 @@ __global__ void __launch_bounds__(32) corridor_walk_kernel(WalkArgs a, const uin
     for (;;) {
         const int64_t r = S[kStR], c = S[kStC];
         if (S[kStDone] || S[kStErr] || r < a.rr0 || c < a.cc0) break;
-        const int64_t bi = (r - a.rr0) / kBR, bj = (c - a.cc0) / kBC;
+        const int64_t bi = (r - a.rr0) / a.br, bj = (c - a.cc0) / kBC;
         if (bi < bi0 || bi >= bi0 + mh || bj < bj0 || bj >= bj0 + mw) break;
         const int32_t slot = map[(bi - bi0) * mw + (bj - bj0)];
         if (slot < 0) break;
-        const int64_t R0 = a.rr0 + bi * kBR, C0 = a.cc0 + bj * kBC;
+        const int64_t R0 = a.rr0 + bi * a.br, C0 = a.cc0 + bj * kBC;
         const int wmax = (int)((r - R0) >> 7);
         const int kn = (int)(c - C0 + 32 < (int64_t)kSteps ? c - C0 + 32 : (int64_t)kSteps);
         const uint32_t chunk = (uint32_t)kn * 32u * 4u;
@@ -656,16 +657,19 @@ int64_t choose_special_interval(const swb_options &opts, int64_t m, int64_t n) {
     return kBR;  // stage 1 keeps every strip's bottom row (512 rows at R = 16)
 }
 
-Plan plan_for(const swb_options &opts, int64_t m, int64_t n) {
+Plan plan_for(const swb_options &opts, int64_t m, int64_t n, int64_t br) {
     Plan p;
+    if (br <= 0 || br > kBR || br % 32 != 0) br = kBR;
     const double budget = (double)(opts.hbm_budget_bytes ? opts.hbm_budget_bytes : (64ULL << 30));
-    const double direct = 8.0 * ((double)(m / kBR) * (double)n + (double)(n / kBC) * (double)m);
+    const double direct = 8.0 * ((double)(m / br) * (double)n + (double)(n / kBC) * (double)m);
     if (direct <= budget) {
         p.level1 = false;
-        p.kr = kBR;
+        p.kr = br;
         p.kc = kBC;
+        p.br = br;
         return p;
     }
+    p.br = kBR;
     // level 1: multiples of the block grid sized to the budget (half rows, half columns)
     p.level1 = true;
     int64_t kr = kBR, kc = kBC;
@@ -675,6 +679,9 @@ Plan plan_for(const swb_options &opts, int64_t m, int64_t n) {
     p.kc = kc;
     return p;
 }
+
+// Block rows of a region's grid: in.br, or the full block height when unset.
+static int64_t block_rows_of(const WalkInputs &in) { return in.br > 0 && in.br <= kBR ? in.br : kBR; }
 
 static WalkArgs to_args(const WalkInputs &in) {
     WalkArgs a{};
@@ -701,6 +708,7 @@ static WalkArgs to_args(const WalkInputs &in) {
     a.xps = in.xps;
     a.xp_cap = in.xp_cap;
     a.st = in.dstate;
+    a.br = (int32_t)block_rows_of(in);
     return a;
 }
 
@@ -710,6 +718,7 @@ static WalkArgs to_args(const WalkInputs &in) {
 // block to the left of each as margin, in walk order, at most `cap` of them.
 static void predict_corridor(const WalkInputs &in, int64_t r, int64_t c, int64_t cap, std::vector<int64_t> &blk,
                              int64_t &bi0, int64_t &bj0, int64_t &mh, int64_t &mw, std::vector<int32_t> &map) {
+    const int64_t BR = block_rows_of(in);
     std::vector<std::pair<int64_t, int64_t>> list;
     auto add = [&](int64_t bi, int64_t bj) {
         if (bi < 0 || bj < 0 || (int64_t)list.size() >= cap) return;
@@ -717,17 +726,17 @@ static void predict_corridor(const WalkInputs &in, int64_t r, int64_t c, int64_t
             if (list[q].first == bi && list[q].second == bj) return;
         list.emplace_back(bi, bj);
     };
-    int64_t bi = (r - in.rr0) / kBR, bj = (c - in.cc0) / kBC;
+    int64_t bi = (r - in.rr0) / BR, bj = (c - in.cc0) / kBC;
     add(bi, bj);
     add(bi - 1, bj);
     add(bi, bj - 1);
     while ((int64_t)list.size() < cap) {
-        const int64_t R0 = in.rr0 + bi * kBR, C0 = in.cc0 + bj * kBC;
+        const int64_t R0 = in.rr0 + bi * BR, C0 = in.cc0 + bj * kBC;
         const int64_t d = std::min(r - R0 + 1, c - C0 + 1);
         r -= d;
         c -= d;
         if (r < in.rr0 || c < in.cc0) break;
-        bi = (r - in.rr0) / kBR;
+        bi = (r - in.rr0) / BR;
         bj = (c - in.cc0) / kBC;
         add(bi, bj);
         add(bi - 1, bj);
@@ -749,7 +758,7 @@ static void predict_corridor(const WalkInputs &in, int64_t r, int64_t c, int64_t
     for (size_t q = 0; q < list.size(); ++q) {
         int32_t &slot = map[(size_t)((list[q].first - bi0) * mw + (list[q].second - bj0))];
         if (slot < 0) slot = (int32_t)q;
-        blk[2 * q] = in.rr0 + list[q].first * kBR;
+        blk[2 * q] = in.rr0 + list[q].first * BR;
         blk[2 * q + 1] = in.cc0 + list[q].second * kBC;
     }
 }

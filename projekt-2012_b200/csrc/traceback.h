@@ -14,10 +14,14 @@ namespace tb {
 // HBM budget and recomputes each level-1 cell on the path.
 struct Plan {
     bool level1 = false;
-    int64_t kr = 512;   // special-row spacing (rows), multiple of 512
+    int64_t kr = 512;   // special-row spacing (rows): br (direct) or a multiple of 512 (level 1)
     int64_t kc = 256;   // special-column spacing (columns), power of two >= 256
+    int64_t br = 512;   // block rows of the walker's grid: the stage-1 strip height in direct
+                        // mode (448 or 512), 512 in level 1
 };
-Plan plan_for(const swb_options &opts, int64_t m, int64_t n);
+// br: the stage-1 strip height the special rows will come from (a multiple of 32
+// up to 512); direct mode when its stores fit the budget.
+Plan plan_for(const swb_options &opts, int64_t m, int64_t n, int64_t br = 512);
 // Level-1 traceback: cells recomputed per corridor round, and device bytes per
 // cell (its 512 x 256 stores and row hand-off buffer).
 int64_t level1_corridor_cells(const Plan &plan, int sms);
@@ -41,6 +45,7 @@ struct WalkInputs {
     int64_t *xps;
     int64_t xp_cap;
     int64_t *dstate;              // device copy of the walker state
+    int64_t br;                   // block rows of the region's grid (0: 512)
 };
 
 

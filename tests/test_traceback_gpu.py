@@ -153,3 +153,14 @@ def test_cli_prints_reference_lines(tmp_path):
     assert "\t>Cell updates per second: " in p.stdout
     assert "Found " in p.stdout and "\t>xPoint[0]: [" in p.stdout
     assert "Visual representation of the alignment" in p.stdout
+
+
+def test_448_row_blocks(gpu_ctx, monkeypatch):
+    """Stage 1 with 448-row strips (14 rows per lane): special rows every 448 rows
+    and the walker's block grid at that spacing give the oracle's alignment."""
+    monkeypatch.setenv("SWB_STAGE1_R", "14")
+    rng = random.Random(31)
+    for m in (700, 2300, 5100):
+        a, b = _similar_pair(rng, m, 0.85)
+        r = _check(gpu_ctx, a, b, (1, -3, -5, -2))
+        assert r.special_interval == 448
