@@ -212,7 +212,7 @@ class Batch:
     swapped: "object"
     traced: "object"
     ops: List[str]             # "" for pairs that were not traced
-    xpoints: List[list]        # [] for pairs that were not traced
+    xpoints: List[list]        # () for pairs that were not traced
     xpoint_interval: "object"
     n_traced: int
     cells: int
@@ -225,13 +225,15 @@ class Batch:
 def _convert_batch(r: BatchResult) -> Batch:
     import numpy as np
     n = r.npairs
-    items = np.ctypeslib.as_array(C.cast(r.items, C.POINTER(C.c_int64)),
-                                 shape=(n * C.sizeof(BatchItem) // 8,)).copy() if n else np.zeros(0, np.int64)
-    raw = items.view(np.uint8).reshape(n, C.sizeof(BatchItem)) if n else np.zeros((0, C.sizeof(BatchItem)), np.uint8)
-    def col(name, dt):
-        off = getattr(BatchItem, name).offset
-        size = np.dtype(dt).itemsize
-        return raw[:, off:off + size].copy().view(dt).reshape(n)
+    size = C.sizeof(BatchItem)
+    ctype_dt = {C.c_int32: np.int32, C.c_int64: np.int64}
+    dt = np.dtype({"names": [f for f, _ in BatchItem._fields_],
+                   "formats": [ctype_dt[t] for _, t in BatchItem._fields_],
+                   "offsets": [getattr(BatchItem, f).offset for f, _ in BatchItem._fields_], "itemsize": size})
+    arr = np.frombuffer(C.string_at(r.items, n * size), dtype=dt) if n else np.zeros(0, dtype=dt)
+
+    def col(name, dtype):
+        return np.array(arr[name], dtype=dtype)
     score, swapped = col("score", np.int32), col("swapped", np.int32)
     traced, xpi = col("traced", np.int32), col("xpoint_interval", np.int32)
     ops_off, n_ops = col("ops_off", np.int64), col("n_ops", np.int64)
@@ -239,11 +241,12 @@ def _convert_batch(r: BatchResult) -> Batch:
     allops = C.string_at(r.ops, r.ops_bytes).decode() if r.ops and r.ops_bytes > 0 else ""
     allxp = _xpoint_tuples(r.xpoints, 0, r.n_xpoints)
     ops = [""] * n
-    xps = [[] for _ in range(n)]
-    for i in np.flatnonzero(traced).tolist():
-        o, x = int(ops_off[i]), int(xp_off[i])
-        ops[i] = allops[o:o + int(n_ops[i])]
-        xps[i] = allxp[x:x + int(n_xp[i])]
+    xps = [()] * n  # one shared empty tuple for the pairs that were not traced
+    idx = np.flatnonzero(traced)
+    for i, o, no, x, nx in zip(idx.tolist(), ops_off[idx].tolist(), n_ops[idx].tolist(), xp_off[idx].tolist(),
+                               n_xp[idx].tolist()):
+        ops[i] = allops[o:o + no]
+        xps[i] = allxp[x:x + nx]
     return Batch(score, col("end_row", np.int64), col("end_col", np.int64), col("start_row", np.int64),
                  col("start_col", np.int64), swapped.astype(bool), traced.astype(bool), ops, xps, xpi,
                  r.n_traced, r.cells, r.stage1_ms, r.stage2_ms, r.total_ms, r.kernel_launches)
@@ -266,9 +269,11 @@ def _xpoint_tuples(ptr, first: int, count: int) -> list:
     import numpy as np
     size = C.sizeof(XPoint)
     raw = C.string_at(C.cast(ptr, C.c_void_p).value + first * size, count * size)
-    a = np.frombuffer(raw, dtype=np.dtype([("gap", np.int32), ("score", np.int32), ("row", np.int64),
-                                           ("col", np.int64)]))
-    return list(zip(a["row"].tolist(), a["col"].tolist(), a["score"].tolist(), a["gap"].tolist()))
+    # the records' fields viewed in (row, col, score, gap) order: tolist() builds the tuples
+    dt = np.dtype({"names": ["row", "col", "score", "gap"], "formats": [np.int64, np.int64, np.int32, np.int32],
+                   "offsets": [XPoint.row.offset, XPoint.col.offset, XPoint.score.offset, XPoint.gap.offset],
+                   "itemsize": size})
+    return np.frombuffer(raw, dtype=dt).tolist()
 
 
 def _convert(r: Result) -> Alignment:
