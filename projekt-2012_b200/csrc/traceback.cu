@@ -11,9 +11,10 @@
 // (X + 1) % (4T) == 0, src/Builders.cpp:16) along that path.  The path does not
 // depend on any tuning parameter of this build.
 //
-// How: stage 1 keeps special rows (H, F) every 512 rows and special columns
-// (H, E) every 256 columns, so every 512 x 256 block of the matrix can be
-// recomputed from its stored boundaries alone, with one direction byte per cell.
+// How: stage 1 keeps special rows (H, F) at every strip bottom (every 448 or 512
+// rows, the strip height) and special columns (H, E) every 256 columns, so every
+// block of that grid (at most 512 x 256) can be recomputed from its stored
+// boundaries alone, with one direction byte per cell.
 // A block's directions do not depend on the path, so the walker of a single
 // pair (walk_region) recomputes a predicted corridor of whole blocks at once,
 // one CTA per block across the GPU (the staircase of blocks along the diagonal
@@ -648,13 +649,6 @@ cudaError_t walker_configure() {
                           cudaFuncSetAttribute((const void *)walk_graph_kernel, A, c)})
         if (x != cudaSuccess) e = x;
     return e;
-}
-
-int64_t choose_special_interval(const swb_options &opts, int64_t m, int64_t n) {
-    (void)opts;
-    (void)m;
-    (void)n;
-    return kBR;  // stage 1 keeps every strip's bottom row (512 rows at R = 16)
 }
 
 Plan plan_for(const swb_options &opts, int64_t m, int64_t n, int64_t br) {

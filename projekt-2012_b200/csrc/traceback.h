@@ -10,8 +10,9 @@ struct GraphHdr;
 namespace tb {
 
 // Special-row / special-column spacing of stage 1 for a pair.  Direct mode keeps
-// the walker's 512 x 256 grid; level-1 mode keeps a coarser grid that fits the
-// HBM budget and recomputes each level-1 cell on the path.
+// the walker's grid (br x 256: the strip height by 256 columns); level-1 mode
+// keeps a coarser grid that fits the HBM budget and recomputes each level-1 cell
+// on the path with 512 x 256 blocks.
 struct Plan {
     bool level1 = false;
     int64_t kr = 512;   // special-row spacing (rows): br (direct) or a multiple of 512 (level 1)
@@ -27,7 +28,6 @@ Plan plan_for(const swb_options &opts, int64_t m, int64_t n, int64_t br = 512);
 int64_t level1_corridor_cells(const Plan &plan, int sms);
 int64_t level1_cell_store_bytes(const Plan &plan);
 cudaError_t walker_configure();
-int64_t choose_special_interval(const swb_options &opts, int64_t m, int64_t n);
 
 // Inputs of one walker launch over a region [rr0, rr1) x [cc0, cc1).
 struct WalkInputs {
