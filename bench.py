@@ -34,7 +34,8 @@ def parse_args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["long", "long200k", "long1mx250k", "tall10mx100k", "small", "chromosome"],
+    p.add_argument("--workload", choices=["long", "long200k", "long1mx250k", "long1mx64k", "tall10mx100k", "small",
+                                          "chromosome"],
                    default="long")
     p.add_argument("--score-only", action="store_true", help="stage 1 only (diagnostics)")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -60,6 +61,11 @@ def workload(name):
         b = b[:250_000]
         desc = ("the 1 Mbp long pair's rows against the first 250 kbp of its columns (same strip "
                 "count and occupancy as the full pair, a quarter of the steps), for profiling")
+    elif name == "long1mx64k":
+        a, b, sc = synth.long_pair()
+        b = b[:65_536]
+        desc = ("the 1 Mbp long pair's rows against the first 65,536 of its columns (same strips and grid as the "
+                "full pair, about 3 GB of special rows and columns), for multi-pass profiles")
     elif name == "tall10mx100k":
         a, b, sc = synth.tall_pair()
         desc = ("10 Mbp iid rows against a mutated 100 kbp window of them (same strip count and occupancy "
