@@ -164,3 +164,8 @@ def test_448_row_blocks(gpu_ctx, monkeypatch):
         a, b = _similar_pair(rng, m, 0.85)
         r = _check(gpu_ctx, a, b, (1, -3, -5, -2))
         assert r.special_interval == 448
+    # more than four byte values: the compare path of the same kernels
+    a, b = _similar_pair(rng, 3000, 0.85)
+    a = a.replace(b"A", b"N", 40)
+    r = _check(gpu_ctx, a, b, (2, -3, -5, -2))
+    assert r.special_interval == 448
