@@ -328,7 +328,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     const bool stores = sr_interval_rows != 0 || sc_interval > 0;
     int R = 16;
     if (const char *rv = std::getenv("SWB_STAGE1_R")) R = std::atoi(rv);  // override: 8, 14, 16 or 32
-    else R = autotune_rows_per_lane(c, a, tab, stores, 16, strip_rows);
+    else R = autotune_rows_per_lane(c, a, tab, stores, 16, strip_rows, sr_interval_rows > 0 ? sr_interval_rows : 0);
     if (strip_rows) {
         if (R != 14 && R != 16) R = 16;
         sr_interval_rows = 32LL * R;

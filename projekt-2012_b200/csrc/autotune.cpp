@@ -73,21 +73,48 @@ void store_locked(const std::string &key, int R) {
 }  // namespace
 
 int autotune_rows_per_lane(swb_ctx *c, const Stage1Args &base, bool tab, bool stores, int fallback,
-                           bool strip_rows) {
+                           bool strip_rows, int64_t sr_interval) {
     // pairs below this many cells are not worth a probe
     constexpr double kMinCells = 2e10;
     if ((double)base.m * (double)base.n < kMinCells) return fallback;
-    const std::string key = key_of(c->sms, stores, tab, base.m, base.n) + (strip_rows ? "|strip" : "");
+    const std::string key = key_of(c->sms, stores, tab, base.m, base.n) + (strip_rows ? "|strip" : "") +
+                            (sr_interval > 0 ? "|sr" + std::to_string(sr_interval) : "");
     {
         std::lock_guard<std::mutex> lk(g_mu);
         load_locked();
         auto it = g_table.find(key);
         if (it != g_table.end()) return it->second;
     }
-    // score only: any height; stores at fixed intervals (level 1): heights that
-    // divide them; stores at every strip bottom (direct traceback): 448 or 512 rows
-    std::vector<int> cands = !stores ? std::vector<int>{8, 14, 16, 32}
-                                     : (strip_rows ? std::vector<int>{14, 16} : std::vector<int>{8, 16});
+    // score only: any height; stores at every strip bottom (direct traceback): 448
+    // or 512 rows; special rows at a fixed interval (level 1): heights that divide it
+    std::vector<int> cands;
+    if (!stores) cands = {8, 14, 16, 32};
+    else if (strip_rows) cands = {14, 16};
+    else
+        for (int R : {8, 14, 16})
+            if (sr_interval <= 0 || sr_interval % (32 * R) == 0) cands.push_back(R);
+    if (cands.empty()) return fallback;
+    if (stores) {
+        // Launches with stores choose between 448- and 512-row strips by how well
+        // the strips fill the resident warps over whole rounds: a probe on a
+        // column slice of a tall pair is dominated by the wavefront's fill, which
+        // favours fewer strips, while the full pair is not.  The store kernel does
+        // about 4% less per cell with 512-row strips, so 448 rows must fill the
+        // warps more than 4% better.  Measured with 448- vs 512-row strips: 1 Mbp
+        // pair 627 vs 667 ms (fill 0.94 vs 0.82), 10 Mbp pair 46.2 vs 45.7 s
+        // (fill 0.94 vs 0.92).
+        auto fill = [&](int R) {
+            const int per_sm = stage1_max_blocks_per_sm(R, tab);
+            const double slots = (double)std::max(1, c->sms) * std::max(1, per_sm) * 4;
+            const double strips = std::ceil((double)base.m / (32.0 * R));
+            return strips / (std::ceil(strips / slots) * slots);
+        };
+        const bool has14 = std::find(cands.begin(), cands.end(), 14) != cands.end();
+        const bool has16 = std::find(cands.begin(), cands.end(), 16) != cands.end();
+        if (has14 && has16) return fill(14) * 0.96 > fill(16) ? 14 : 16;
+        if (has16) return 16;
+        if (has14) return 14;
+    }
     const int64_t np = std::min<int64_t>(base.n, 1 << 18);
     int bestR = fallback;
     float bestMs = 1e30f;

@@ -106,7 +106,8 @@ cudaError_t ctx_put(swb_ctx *c, void *dev_dst, const void *src, size_t bytes);
 // pair described by `base` (rows, columns, encodings, scoring and the hand-off,
 // best and error buffers must be set).  Small pairs get `fallback`.
 // strip_rows: special rows at every strip bottom, height 448 or 512 rows.
+// sr_interval: special rows every that many rows (level 1), 0 for none.
 int autotune_rows_per_lane(swb_ctx *c, const Stage1Args &base, bool tab, bool stores, int fallback,
-                           bool strip_rows = false);
+                           bool strip_rows = false, int64_t sr_interval = 0);
 
 }  // namespace swb

@@ -664,9 +664,12 @@ Plan plan_for(const swb_options &opts, int64_t m, int64_t n, int64_t br) {
         return p;
     }
     p.br = kBR;
-    // level 1: multiples of the block grid sized to the budget (half rows, half columns)
+    // level 1: multiples of the block grid sized to the budget (half rows, half
+    // columns).  The row spacing starts at 3584 = 7 x 512 = 8 x 448 rows, so stage
+    // 1 may run 448-row strips as well as 512- or 256-row ones, while each level-1
+    // cell is recomputed with 512-row blocks.
     p.level1 = true;
-    int64_t kr = kBR, kc = kBC;
+    int64_t kr = 7 * kBR, kc = kBC;
     while (8.0 * (double)(m / kr) * (double)n > budget / 2) kr *= 2;
     while (8.0 * (double)(n / kc) * (double)m > budget / 2) kc *= 2;
     p.kr = kr;

@@ -15,7 +15,7 @@ namespace tb {
 // on the path with 512 x 256 blocks.
 struct Plan {
     bool level1 = false;
-    int64_t kr = 512;   // special-row spacing (rows): br (direct) or a multiple of 512 (level 1)
+    int64_t kr = 512;   // special-row spacing (rows): br (direct) or 3584 x 2^k (level 1)
     int64_t kc = 256;   // special-column spacing (columns), power of two >= 256
     int64_t br = 512;   // block rows of the walker's grid: the stage-1 strip height in direct
                         // mode (448 or 512), 512 in level 1
