@@ -167,6 +167,11 @@ int swb_ctx_create(const swb_options *opts, swb_ctx **out) {
         (e = swb::stage1_configure()) != cudaSuccess || (e = swb::batch_configure()) != cudaSuccess ||
         (e = swb::tb::walker_configure()) != cudaSuccess) {
         int rc = ctx_cuda_fail(nullptr, e, "swb_ctx_create");
+        // release what was created before the failure
+        if (c->ev0) cudaEventDestroy(c->ev0);
+        if (c->ev1) cudaEventDestroy(c->ev1);
+        if (c->ev2) cudaEventDestroy(c->ev2);
+        if (c->stream && c->opts.cuda_stream == 0) cudaStreamDestroy(c->stream);
         delete c;
         return rc;
     }
