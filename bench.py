@@ -399,6 +399,7 @@ def main():
     import torch
     import torch.distributed as dist
     import swb200
+    from swb200.ranks import max_over_ranks, replica_throughput
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -447,9 +448,7 @@ def main():
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = max_over_ranks(ms, "cuda")
             dist.barrier()
         return ms, res
 
@@ -460,8 +459,8 @@ def main():
     for r in res_dev + res_e2e:
         assert (r.score, r.end_row, r.end_col) == (first.score, first.end_row, first.end_col)
 
-    value = world * cells * args.steps / (ms_dev * 1e-3) / 1e9
-    e2e = world * cells * args.steps / (ms_e2e * 1e-3) / 1e9
+    value = replica_throughput(world, cells, args.steps, ms_dev) / 1e9
+    e2e = replica_throughput(world, cells, args.steps, ms_e2e) / 1e9
     k_ms = sum(r.stage1_ms for r in res_dev) / len(res_dev)
     achieved = cells / (k_ms * 1e-3) / 1e9
     peak_cells = swb200.probe_cell_peak(local)
