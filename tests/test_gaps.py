@@ -117,3 +117,31 @@ def test_gap_lists_reject_bad_operations():
     with pytest.raises(swb200.SwbError) as ei:
         swb200.gap_lists(types.SimpleNamespace(ops="MMXM", start_row=0, start_col=0))
     assert ei.value.code == swb200.SWB_EINVAL
+
+
+def _ops_strategy():
+    from hypothesis import strategies as st
+    run = st.tuples(st.sampled_from("MID"), st.integers(1, 9))
+    return st.lists(run, min_size=0, max_size=30).map(lambda rs: "M" + "".join(o * k for o, k in rs) + "M")
+
+
+def test_gap_lists_round_trip_property():
+    from hypothesis import given, settings
+    from hypothesis import strategies as st
+
+    @settings(max_examples=150, deadline=None)
+    @given(_ops_strategy(), st.integers(0, 40), st.integers(0, 40), st.integers(0, 2**31 - 1))
+    def check(ops, sr, sc, seed):
+        rng = random.Random(seed)
+        nr, nc = sr + ops.count("M") + ops.count("D") + 5, sc + ops.count("M") + ops.count("I") + 5
+        rows = bytes(rng.choice(b"ACGT") for _ in range(nr))
+        cols = bytes(rng.choice(b"ACGT") for _ in range(nc))
+        er = sr + ops.count("M") + ops.count("D") - 1
+        ec = sc + ops.count("M") + ops.count("I") - 1
+        al = types.SimpleNamespace(ops=ops, start_row=sr, start_col=sc)
+        g1, g2 = swb200.gap_lists(al)
+        assert all(L > 0 for _, L in g1 + g2)
+        assert [b for b, _ in g1] == sorted(b for b, _ in g1) and [b for b, _ in g2] == sorted(b for b, _ in g2)
+        assert _visual_output(rows, cols, g1, g2, (sr, sc), (er, ec)) == _render_ops(rows, cols, ops, sr, sc)
+
+    check()
