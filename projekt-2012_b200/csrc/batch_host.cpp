@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include "batch.h"
@@ -147,6 +148,26 @@ void layout_stores(std::vector<BatchPair> &bp, const swb_batch_item *items, cons
     }
 }
 
+
+// Host copy into pinned staging, split over a few threads for large buffers
+// (one core copies ~10 GB/s; the batch's sequences are tens of MB).
+void copy_parallel(uint8_t *dst, const uint8_t *src, size_t bytes) {
+    constexpr size_t kChunk = 8u << 20;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t parts = std::min<size_t>(std::min<size_t>(8, hw), (bytes + kChunk - 1) / kChunk);
+    if (parts <= 1) {
+        if (bytes) std::memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t per = (bytes + parts - 1) / parts;
+    std::vector<std::thread> th;
+    for (size_t k = 1; k < parts; ++k) {
+        const size_t lo = k * per, n = lo < bytes ? std::min(per, bytes - lo) : 0;
+        if (n) th.emplace_back([=] { std::memcpy(dst + lo, src + lo, n); });
+    }
+    std::memcpy(dst, src, std::min(per, bytes));
+    for (auto &t : th) t.join();
+}
 
 bool graphs_enabled() {
     const char *v = std::getenv("SWB_BATCH_GRAPH");
@@ -412,7 +433,7 @@ int graph_pass(swb_ctx *c, const uint8_t *h_seq, int64_t seq_bytes, const std::v
         }
         tb::pack_walk_args(win.data(), np, g.walk_states, hin + in_walk);
     }
-    if (seq_bytes > 0) std::memcpy(hin + in_seq, h_seq, (size_t)seq_bytes);
+    copy_parallel(hin + in_seq, h_seq, (size_t)seq_bytes);
     // size class: the smallest power of two >= the unit count (pairs <= units), up
     // to one that no longer shrinks any grid
     int size_class = 0;
@@ -631,10 +652,13 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
         stores_first ? npairs : std::min<int64_t>(npairs, (int64_t)std::ceil(trace_frac * (double)npairs - 1e-9));
     if (ntrace > 0) {
         const auto t1 = std::chrono::steady_clock::now();
+        // the ntrace best scores (ties: lower index first)
         std::vector<int64_t> byscore((size_t)npairs);
         std::iota(byscore.begin(), byscore.end(), 0);
-        std::stable_sort(byscore.begin(), byscore.end(),
-                         [&](int64_t x, int64_t y) { return out->items[x].score > out->items[y].score; });
+        std::partial_sort(byscore.begin(), byscore.begin() + ntrace, byscore.end(), [&](int64_t x, int64_t y) {
+            const int32_t sx = out->items[x].score, sy = out->items[y].score;
+            return sx != sy ? sx > sy : x < y;
+        });
         byscore.resize((size_t)ntrace);
         std::sort(byscore.begin(), byscore.end());
         std::vector<int64_t> tr;  // traced pairs that have an alignment (score > 0)
