@@ -66,6 +66,11 @@ typedef struct {
 #define SWB_FLAG_TIE_ROWMAJOR  0x1u  /* default is SWB_TIE_REFERENCE              */
 #define SWB_FLAG_SCORE_ONLY    0x2u  /* score and end cell only (stage 1)          */
 #define SWB_FLAG_NO_SPECIAL    0x4u  /* stage 1 without special-row checkpoints    */
+/* Test hook of swb_align_pair[_device]: strip 0 never hands its bottom row to
+ * strip 1, so strip 1's first wait runs out after wait_limit_ms and the call
+ * returns SWB_ETIMEOUT with the context still usable.  Pairs of one strip (at
+ * most 448 rows) have no wait and are unaffected. */
+#define SWB_FLAG_TEST_WITHHOLD 0x80000000u
 
 typedef struct {
     int32_t score;
@@ -100,6 +105,11 @@ typedef struct {
                                        the stage-1 strip trace (swb_trace_copy)     */
     uint64_t cuda_stream;           /* a cudaStream_t of the caller to run on, cast
                                        to an integer; 0 = the context's own stream */
+    uint32_t wait_limit_ms;         /* bound of every wait of one strip for the strip
+                                       above on the GPU; past it the launch stops
+                                       and the call returns SWB_ETIMEOUT (the
+                                       reference exits -2 on any CUDA error,
+                                       src/SWutils.cpp:19-24); 0 = 20,000 ms      */
 } swb_options;
 
 typedef struct swb_ctx swb_ctx;
@@ -316,7 +326,8 @@ int swb_gap_lists_write(const swb_result *result, const char *first_path, const 
  * '>'; the name is the first line without '>' and its last character (at most
  * 199 bytes read); the first 299 bytes of that line are skipped; every other
  * byte except '
-' and '' is sequence, unchanged.  With SWB_FASTA_MULTI every
+' and '
+' is sequence, unchanged.  With SWB_FASTA_MULTI every
  * line starting with '>' opens a record whose name is that whole line (any
  * length, without '>' and the line end), lines starting with ';' are comments,
  * and blanks, tabs and line ends are dropped from sequences.  SWB_FASTA_UPPER

@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(HERE, "build", "liboracle.so")
 REFEMU_PATH = os.path.join(HERE, "_ref", "swalign_emu")
 
 TEXTBOOK, SHIPPED_CARRY = 0, 1
-TIE_REFERENCE, TIE_ROWMAJOR = 0, 1
+TIE_REFERENCE, TIE_ROWMAJOR, TIE_BOTH = 0, 1, 2
 
 
 class Scoring(C.Structure):
@@ -54,6 +54,8 @@ def lib():
         L.orc_stage1_mt.argtypes = [u8p, C.c_int64, u8p, C.c_int64, C.POINTER(Scoring),
                                     C.c_int, C.c_int, C.POINTER(End), C.POINTER(C.c_int64)]
         L.orc_stage1_mt.restype = C.c_int
+        L.orc_stage1_simd.argtypes = L.orc_stage1_mt.argtypes
+        L.orc_stage1_simd.restype = C.c_int
         L.orc_special_rows.argtypes = [u8p, C.c_int64, u8p, C.c_int64, C.POINTER(Scoring),
                                        C.c_int64, C.c_void_p, C.c_int64]
         L.orc_special_rows.restype = C.c_int64
@@ -69,6 +71,9 @@ def lib():
         L.orc_score_ops.argtypes = [u8p, u8p, C.POINTER(Scoring), C.c_int64, C.c_int64,
                                     C.c_char_p, C.c_int64]
         L.orc_score_ops.restype = C.c_int64
+        L.orc_anchored_score.argtypes = [u8p, C.c_int64, u8p, C.c_int64, C.POINTER(Scoring),
+                                         C.c_int64, C.c_int64, C.c_int64, C.c_int64]
+        L.orc_anchored_score.restype = C.c_int64
         _lib = L
     return _lib
 
@@ -117,6 +122,44 @@ def stage1_mt(rows: bytes, cols: bytes, sc: Scoring, tie=TIE_REFERENCE, threads=
     return Stage1(e.score, e.row, e.col), ns.value * 1e-9
 
 
+def stage1_simd(rows: bytes, cols: bytes, sc: Scoring, tie=TIE_REFERENCE, threads=None):
+    """Returns (Stage1, seconds) from the AVX-512 wavefront, or None when the CPU
+    has no AVX-512."""
+    threads = threads or os.cpu_count() or 1
+    e = End()
+    ns = C.c_int64(0)
+    rc = lib().orc_stage1_simd(rows, len(rows), cols, len(cols), C.byref(sc), tie, threads,
+                               C.byref(e), C.byref(ns))
+    if rc == -4:
+        return None
+    if rc != 0:
+        raise RuntimeError(f"orc_stage1_simd failed: {rc}")
+    return Stage1(e.score, e.row, e.col), ns.value * 1e-9
+
+
+def stage1_simd_both(rows: bytes, cols: bytes, sc: Scoring, threads=None):
+    """Both tie rules in one AVX-512 pass: ((reference, rowmajor), seconds) or None."""
+    threads = threads or os.cpu_count() or 1
+    e = (End * 2)()
+    ns = C.c_int64(0)
+    rc = lib().orc_stage1_simd(rows, len(rows), cols, len(cols), C.byref(sc), TIE_BOTH, threads,
+                               e, C.byref(ns))
+    if rc == -4:
+        return None
+    if rc != 0:
+        raise RuntimeError(f"orc_stage1_simd failed: {rc}")
+    return (Stage1(e[0].score, e[0].row, e[0].col), Stage1(e[1].score, e[1].row, e[1].col)), ns.value * 1e-9
+
+
+def stage1_fast(rows: bytes, cols: bytes, sc: Scoring, tie=TIE_REFERENCE, threads=None):
+    """The fastest multithreaded stage 1 this CPU runs: (Stage1, seconds, kind)."""
+    r = stage1_simd(rows, cols, sc, tie, threads)
+    if r is not None:
+        return r[0], r[1], "avx512"
+    s, t = stage1_mt(rows, cols, sc, tie, threads)
+    return s, t, "scalar"
+
+
 def special_rows(rows: bytes, cols: bytes, sc: Scoring, k: int):
     import numpy as np
     nrows = len(rows) // k
@@ -157,6 +200,11 @@ def traceback_xp(rows: bytes, cols: bytes, sc: Scoring, er: int, ec: int, interv
 def score_ops(rows: bytes, cols: bytes, sc: Scoring, sr: int, scol: int, ops: str) -> int:
     o = ops.encode()
     return lib().orc_score_ops(rows, cols, C.byref(sc), sr, scol, o, len(o))
+
+
+def anchored_score(rows: bytes, cols: bytes, sc: Scoring, sr: int, scol: int, er: int, ec: int) -> int:
+    """Best score of an alignment from the diagonal cell (sr, scol) to (er, ec)."""
+    return lib().orc_anchored_score(rows, len(rows), cols, len(cols), C.byref(sc), sr, scol, er, ec)
 
 
 def crosspoints(ops: str, sr: int, scol: int, interval: int):

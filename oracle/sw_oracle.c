@@ -499,3 +499,39 @@ int64_t orc_score_ops(const uint8_t *a, const uint8_t *b, const orc_scoring *sc,
     }
     return s;
 }
+
+/* Best score of an alignment whose first cell is the diagonal cell (sr, sc_) and
+ * whose last cell is (er, ec), with the same gap recurrence as stage 1 but no
+ * zero floor: a start cell found by some other search is the start of an optimal
+ * local alignment ending at (er, ec) exactly when this equals the best score. */
+int64_t orc_anchored_score(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
+                           const orc_scoring *sc, int64_t sr, int64_t sc_, int64_t er, int64_t ec) {
+    if (sr < 0 || sc_ < 0 || er < sr || ec < sc_ || er >= m || ec >= n) return INT64_MIN;
+    const int64_t W = ec - sc_ + 1;
+    const int64_t NEG = INT64_MIN / 4;
+    int64_t *H = malloc(sizeof(int64_t) * (size_t)W), *F = malloc(sizeof(int64_t) * (size_t)W);
+    if (!H || !F) { free(H); free(F); return INT64_MIN; }
+    for (int64_t j = 0; j < W; ++j) { H[j] = NEG; F[j] = NEG; }
+    for (int64_t i = sr; i <= er; ++i) {
+        int64_t hl = NEG, el = NEG, hd = NEG;
+        for (int64_t j = 0; j < W; ++j) {
+            const int64_t s = (a[i] == b[sc_ + j]) ? sc->match : sc->mismatch;
+            const int64_t f = (i > sr) ? (F[j] + sc->gap_extend > H[j] + sc->gap_open ? F[j] + sc->gap_extend
+                                                                                      : H[j] + sc->gap_open) : NEG;
+            const int64_t e = (j > 0) ? (el + sc->gap_extend > hl + sc->gap_open ? el + sc->gap_extend
+                                                                                : hl + sc->gap_open) : NEG;
+            int64_t h = (i == sr && j == 0) ? s : hd + s;
+            if (e > h) h = e;
+            if (f > h) h = f;
+            if (h < NEG / 2) h = NEG;
+            hd = H[j];
+            H[j] = h;
+            F[j] = f < NEG / 2 ? NEG : f;
+            hl = h;
+            el = e < NEG / 2 ? NEG : e;
+        }
+    }
+    const int64_t res = H[W - 1];
+    free(H); free(F);
+    return res;
+}

@@ -36,7 +36,8 @@ typedef struct {
 enum { ORC_TEXTBOOK = 0,    /* zero boundaries: the H matrix of textbook Gotoh SW */
        ORC_SHIPPED_CARRY = 1 /* the shipped kernels' left boundary carry (see .c)  */ };
 enum { ORC_TIE_REFERENCE = 0, /* the shipped kernels' thread-ownership order      */
-       ORC_TIE_ROWMAJOR = 1 };
+       ORC_TIE_ROWMAJOR = 1,
+       ORC_TIE_BOTH = 2 };    /* orc_stage1_simd only: out[0] reference, out[1] row-major */
 
 /* Returns 0, or -1 when the reference cannot launch (shorter length < 4). */
 int orc_geometry(int64_t rows, int64_t cols, orc_geom *g);
@@ -54,6 +55,14 @@ int orc_stage1(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
  * *ns_out when it is not NULL. */
 int orc_stage1_mt(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
                   const orc_scoring *sc, int tie, int threads, orc_end *out, int64_t *ns_out);
+
+/* The same result as orc_stage1_mt() from an AVX-512 anti-diagonal wavefront
+ * (sw_oracle_simd.c): strips of 16 rows, one row per vector lane.  With tie =
+ * ORC_TIE_BOTH, out points to two results (reference order, row-major) found in
+ * one pass.  Returns -4 when the CPU has no AVX-512 (callers then use
+ * orc_stage1_mt). */
+int orc_stage1_simd(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
+                    const orc_scoring *sc, int tie, int threads, orc_end *out, int64_t *ns_out);
 
 /* Full H/E/F rows for checking special rows: writes H and F of every row r with
  * (r + 1) % k == 0 into hf[(r + 1) / k - 1][c] as (H, F) pairs (textbook).
@@ -87,6 +96,13 @@ int64_t orc_traceback_xp(const uint8_t *a, int64_t m, const uint8_t *b, int64_t 
  * gap_extend), which is what the recurrence gives. */
 int64_t orc_score_ops(const uint8_t *a, const uint8_t *b, const orc_scoring *sc,
                       int64_t sr, int64_t sc_, const char *ops, int64_t nops);
+
+/* Best score of an alignment that starts with the diagonal cell (sr, sc_) and ends
+ * at (er, ec) (same gap recurrence, no zero floor); INT64_MIN on bad input.  Used
+ * to check that a start cell reported by the reference's own stage 2 begins an
+ * optimal alignment. */
+int64_t orc_anchored_score(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
+                           const orc_scoring *sc, int64_t sr, int64_t sc_, int64_t er, int64_t ec);
 
 #ifdef __cplusplus
 }

@@ -179,6 +179,11 @@ int swb_ctx_create(const swb_options *opts, swb_ctx **out) {
         c->stream = (cudaStream_t)(uintptr_t)c->opts.cuda_stream;
         c->own_stream = false;
     }
+    if (c->opts.wait_limit_ms > 0) {
+        int khz = 0;  // the kernels bound their waits with clock64(), in SM cycles
+        if (cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, c->device) != cudaSuccess || khz <= 0) khz = 2000000;
+        c->wait_cycles = (int64_t)c->opts.wait_limit_ms * khz;
+    }
     c->each_buf([c](DevBuf &b) { b.st = c->stream; });
     *out = c;
     return SWB_OK;
@@ -317,6 +322,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     a.best = (BestRec *)c->best.p;
     a.err = (int32_t *)c->errf.p;
     a.gbest = a.err + 2;
+    a.wait_limit = c->wait_cycles;
     int32_t G = 0, T = 0;
     int64_t P1 = 0, P2 = 0;
     const bool refok = reference_geometry(m, n, &G, &T, &P1, &P2);
@@ -398,6 +404,7 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     if ((e = cudaMemsetAsync(a.hbuf, 0xFF, sizeof(int4) * (size_t)n, c->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(a.err, 0, 4 * sizeof(int32_t), c->stream)) != cudaSuccess)
         return ctx_cuda_fail(c, e, "stage 1 reset");
+    a.withhold = (flags & SWB_FLAG_TEST_WITHHOLD) ? 1 : 0;  // set after the autotuner's probes
     cudaEventRecord(c->ev0, c->stream);
     if ((e = stage1_launch(a, plan, c->stream)) != cudaSuccess) return ctx_cuda_fail(c, e, "stage 1 launch");
     cudaEventRecord(c->ev1, c->stream);

@@ -73,6 +73,8 @@ struct PairView : S {
     int4 *hbuf;
     int32_t *gbest;
     TieGeom tie;
+    int64_t wait_limit;
+    static constexpr int32_t withhold = 0;
     static constexpr int64_t r_origin = 0;
     static constexpr int64_t c_origin = 0;
     static constexpr int64_t *trace = nullptr;
@@ -111,6 +113,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs &g) {
         v.hbuf = g.hbuf + d.hbuf_off;
         v.gbest = g.gbest + d.slot;
         v.tie = d.tie;
+        v.wait_limit = g.wait_limit;
         if constexpr (!std::is_same<S, NoStores>::value) {
             v.srows = g.srows + d.sr_off;
             v.sr_every = d.sr_every;

@@ -52,6 +52,7 @@ struct BatchArgs {
     BestRec *ubest;            // per work unit: best cell of that strip
     int32_t *ctl;              // [0] unit counter, [1] error code, [2] abort flag
     int2 *srows, *scols;       // store pass: special rows (H, F) / columns (H, E) of every pair
+    int64_t wait_limit;        // bound of each wait for the strip above, in SM clock cycles; 0 = default
 };
 
 // Rows per lane of the batched kernel's store passes (their strips are 512 rows,

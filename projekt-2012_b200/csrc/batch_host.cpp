@@ -393,6 +393,7 @@ int graph_pass(swb_ctx *c, const uint8_t *h_seq, int64_t seq_bytes, const std::v
     g.ba.gbest = (int32_t *)(dw + w_gbest);
     g.ba.ubest = (BestRec *)(dw + w_ubest);
     g.ba.ctl = (int32_t *)(dout + o_ctl);
+    g.ba.wait_limit = c->wait_cycles;
     g.ba.srows = traced ? (int2 *)(dw + w_srows) : nullptr;
     g.ba.scols = traced ? (int2 *)(dw + w_scols) : nullptr;
     g.pbest = (BestRec *)(dout + o_pbest);
@@ -554,6 +555,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
     }
 
     BatchArgs base{};
+    base.wait_limit = c->wait_cycles;
     base.open = sc->gap_open;
     base.ext = sc->gap_extend;
     base.gx = std::max(sc->gap_open, sc->gap_extend);

@@ -39,6 +39,7 @@ struct swb_ctx {
     cudaStream_t stream = nullptr;
     bool own_stream = true;
     int sms = 0;
+    int64_t wait_cycles = 0;  // opts.wait_limit_ms in SM clock cycles (0: the kernels' default)
     std::string err;
     swb::DevBuf rows, cols, hbuf, wbest, best, errf, srows, scols, work, flags, lut, rcode, ctab, trace;
     swb::DevBuf tb[24];  // traceback scratch (ops, crosspoints, state, level-2 stores, recompute and walker buffers)

@@ -27,7 +27,7 @@ constexpr int kCH = 8;         // steps per refill
 constexpr int kRing = 32;      // ring entries per warp
 constexpr int kStage = 16;     // staged bottom-row entries per warp (flushed every refill)
 constexpr int kWarps = 4;      // warps per block
-constexpr long long kWaitLimitCycles = 40LL * 1000 * 1000 * 1000;  // bound of every wait (~20 s)
+constexpr long long kWaitLimitCycles = 40LL * 1000 * 1000 * 1000;  // default bound of every wait (~20 s)
 
 enum : int32_t { kErrNone = 0, kErrTimeout = 4 };
 
@@ -262,11 +262,12 @@ template <class A>
 __device__ __forceinline__ bool commit(const A &a, int4 *ring, int32_t strip, int32_t c, Pre &p) {
     if (strip > 0 && (p.h.y != strip - 1 || p.h.w != strip - 1)) {
         const long long t0 = clock64();
+        const long long limit = a.wait_limit > 0 ? a.wait_limit : kWaitLimitCycles;
         for (;;) {
             __nanosleep(32);
             p.h = ld_ll(a.hbuf + c);
             if (p.h.y == strip - 1 && p.h.w == strip - 1) break;
-            if (ld_volatile(&a.err[1]) != 0 || clock64() - t0 > kWaitLimitCycles) return false;
+            if (ld_volatile(&a.err[1]) != 0 || clock64() - t0 > limit) return false;
         }
     }
     ring[c & (kRing - 1)] = make_int4(p.h.x, p.h.z, (int32_t)p.cv, 0);
@@ -326,7 +327,7 @@ __device__ bool run_strip(const A &a, int4 *ring, int4 *stage, int lane, int32_t
     sc.row0 = (int64_t)s * H + (int64_t)lane * R;
     sc.strip = s;
     sc.n = (int32_t)a.n;
-    sc.below = (int64_t)(s + 1) * H < a.m;
+    sc.below = (int64_t)(s + 1) * H < a.m && !(a.withhold && s == 0);
     sc.sr = a.srows != nullptr && ((int64_t)(s + 1) % a.sr_every) == 0 && (int64_t)(s + 1) * H <= a.m;
     sc.sr_off = sc.sr ? ((int64_t)(s + 1) / a.sr_every - 1) * a.n : 0;
     L.bho = bho;

@@ -63,6 +63,8 @@ struct Stage1Args {
     int32_t *gbest;        // best H seen so far in this matrix (err + 2 for a single pair)
     int64_t *trace;        // optional: per strip {start ns, end ns, SM id} (globaltimer)
     TieGeom tie;
+    int64_t wait_limit;    // bound of each wait for the strip above, in SM clock cycles; 0 = kWaitLimitCycles
+    int32_t withhold;      // test hook: strip 0 writes no hand-off entries (SWB_FLAG_TEST_WITHHOLD)
 };
 
 // Geometry of the reference's launch (src/SWutils.cpp:233-253) and padding

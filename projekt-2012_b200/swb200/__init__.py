@@ -28,6 +28,7 @@ SWB_ENOTFOUND = 8
 FLAG_TIE_ROWMAJOR = 0x1
 FLAG_SCORE_ONLY = 0x2
 FLAG_NO_SPECIAL = 0x4
+FLAG_TEST_WITHHOLD = 0x80000000  # test hook (include/swb200.h)
 
 
 class Scoring(C.Structure):
@@ -93,7 +94,7 @@ class ServerStats(C.Structure):
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64),
                 ("special_interval", C.c_int32), ("verbose", C.c_int32),
-                ("cuda_stream", C.c_uint64)]
+                ("cuda_stream", C.c_uint64), ("wait_limit_ms", C.c_uint32)]
 
 
 class SwbError(RuntimeError):
@@ -358,7 +359,7 @@ class Context:
     """One device context (owns a CUDA stream and reusable device buffers)."""
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, special_interval: int = 0,
-                 cuda_stream: int = 0, verbose: int = 0):
+                 cuda_stream: int = 0, verbose: int = 0, wait_limit_ms: int = 0):
         L = lib()
         o = Options()
         L.swb_options_default(C.byref(o))
@@ -367,6 +368,7 @@ class Context:
         o.special_interval = special_interval
         o.cuda_stream = cuda_stream
         o.verbose = verbose
+        o.wait_limit_ms = wait_limit_ms
         h = C.c_void_p()
         rc = L.swb_ctx_create(C.byref(o), C.byref(h))
         if rc != SWB_OK:

@@ -131,3 +131,62 @@ def test_traceback_scores_and_bounds():
         assert O.score_ops(rows, cols, sc, sr, sc_, ops) == r.score
         assert sr + ops.count("M") + ops.count("D") - 1 == r.row
         assert sc_ + ops.count("M") + ops.count("I") - 1 == r.col
+
+
+def _simd_available():
+    return O.stage1_simd(b"ACGT", b"ACG", O.scoring(1, -3, -5, -2), threads=1) is not None
+
+
+@pytest.mark.skipif(not _simd_available(), reason="CPU without AVX-512")
+def test_simd_wavefront_equals_scalar_oracle():
+    """orc_stage1_simd (16-row strips, one row per lane, blocks handed between
+    threads) gives the scalar oracle's score and end cell under both tie rules,
+    on ragged sizes around the strip height and the column block width."""
+    rng = random.Random(31)
+    for _ in range(160):
+        alph = rng.choice([b"ACGT", b"AC", b"A", b"ACGTN"])
+        m = rng.choice([1, 2, 15, 16, 17, 33, 100, 1000, 4097])
+        n = rng.choice([1, 3, 14, 15, 16, 17, 300, 4095, 4097, 8200])
+        a = bytes(rng.choice(alph) for _ in range(m))
+        if rng.random() < 0.5 and n <= m:
+            st = rng.randint(0, m - n)
+            b = bytes(c if rng.random() > 0.1 else rng.choice(alph) for c in a[st:st + n])
+        else:
+            b = bytes(rng.choice(alph) for _ in range(n))
+        rows, cols, _ = O.orient(a, b)
+        sc = O.scoring(*rng.choice([(1, -3, -5, -2), (5, -5, -5, -5), (2, -3, -5, -2), (1, -1, -1, -1)]))
+        (r0, r1), _ = O.stage1_simd_both(rows, cols, sc, threads=rng.choice([1, 2, 5, 8]))
+        e0 = O.stage1(rows, cols, sc, O.TEXTBOOK, O.TIE_REFERENCE)
+        e1 = O.stage1(rows, cols, sc, O.TEXTBOOK, O.TIE_ROWMAJOR)
+        assert (r0.score, r0.row, r0.col) == (e0.score, e0.row, e0.col), (m, n)
+        assert (r1.score, r1.row, r1.col) == (e1.score, e1.row, e1.col), (m, n)
+
+
+@pytest.mark.skipif(not _simd_available(), reason="CPU without AVX-512")
+def test_simd_wavefront_on_test3_golden(goldens):
+    """The reference's Tests/test3.sh golden (2.8e10 cells) through the AVX-512 wavefront."""
+    g = goldens[2]
+    a, b = load_fixture_fasta(g["a"]), load_fixture_fasta(g["b"])
+    rows, cols, _ = O.orient(a, b)
+    r, _ = O.stage1_simd(rows, cols, O.scoring(*g["scoring"]))
+    assert (r.score, r.row + 1, r.col + 1) == (g["score"], g["row1"], g["col1"])
+
+
+def test_anchored_score_from_the_canonical_start():
+    """An alignment from the canonical traceback's start cell to the end cell
+    scores exactly the best score; one cell to the right of the start it can
+    only score less or the same."""
+    rng = random.Random(5)
+    for _ in range(40):
+        a = bytes(rng.choice(b"ACGT") for _ in range(rng.randint(20, 150)))
+        b = bytes(c if rng.random() > 0.1 else rng.choice(b"ACGT") for c in a[5:rng.randint(20, len(a))])
+        rows, cols, _ = O.orient(a, b)
+        sc = O.scoring(*rng.choice([(1, -3, -5, -2), (5, -5, -5, -5), (1, -1, -1, -1)]))
+        e = O.stage1(rows, cols, sc)
+        if e.score == 0:
+            continue
+        ops, sr, scol = O.traceback(rows, cols, sc, e.row, e.col)
+        assert O.anchored_score(rows, cols, sc, sr, scol, e.row, e.col) == e.score
+        if scol + 1 <= e.col:
+            assert O.anchored_score(rows, cols, sc, sr, scol + 1, e.row, e.col) <= e.score
+    assert O.anchored_score(b"AC", b"AC", sc, 1, 1, 0, 0) == -(2 ** 63)

@@ -125,3 +125,28 @@ def test_special_rows_match_oracle():
             got, interval = ctx.special_row(i, len(cols))
             assert interval == 1024
             np.testing.assert_array_equal(got, ref[i])
+
+
+def test_bounded_wait_runs_out_and_the_context_stays_usable():
+    """A strip whose wait for the strip above runs out ends the launch: the call
+    returns SWB_ETIMEOUT (the reference would exit -2, src/SWutils.cpp:19-24) within
+    the context's wait limit, every other warp stops at its next wait, and the next
+    call on the same context returns the oracle's result.  The stall is made on the
+    host side of the kernel's contract: the test flag keeps strip 0 from writing
+    its hand-off entries, so nothing ever satisfies strip 1's wait."""
+    import time
+    rng = random.Random(3)
+    a = bytes(rng.choice(b"ACGT") for _ in range(6000))  # 6,000 rows: 12+ strips
+    b = bytes(rng.choice(b"ACGT") for _ in range(2500))
+    sc_t = (1, -3, -5, -2)
+    rows, cols, _ = O.orient(a, b)
+    e = O.stage1(rows, cols, O.scoring(*sc_t), O.TEXTBOOK, O.TIE_REFERENCE)
+    with swb200.Context(device=0, wait_limit_ms=200) as ctx:
+        for flags in (swb200.FLAG_SCORE_ONLY, 0):
+            t0 = time.monotonic()
+            with pytest.raises(swb200.SwbError) as ei:
+                ctx.align(a, b, swb200.scoring(*sc_t), flags | swb200.FLAG_TEST_WITHHOLD)
+            assert ei.value.code == swb200.SWB_ETIMEOUT
+            assert time.monotonic() - t0 < 10.0
+            r = ctx.align(a, b, swb200.scoring(*sc_t), flags)
+            assert (r.score, r.end_row, r.end_col) == (e.score, e.row, e.col)
