@@ -8,12 +8,14 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import struct
 import subprocess
 from dataclasses import dataclass
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "build", "liboracle.so")
 REFEMU_PATH = os.path.join(HERE, "_ref", "swalign_emu")
+VISUAL_PATH = os.path.join(HERE, "_ref", "visual_emu")
 
 TEXTBOOK, SHIPPED_CARRY = 0, 1
 TIE_REFERENCE, TIE_ROWMAJOR, TIE_BOTH = 0, 1, 2
@@ -254,3 +256,30 @@ def run_reference(fa: str, fb: str, match: int, mismatch: int, gap_open: int, ga
             elif f[1] == "xpoint":
                 res["xpoints"].append(tuple(int(x) for x in f[3:7]))
     return res
+
+
+def run_reference_visual(first: bytes, second: bytes, first_gaps: str, second_gaps: str, start, end,
+                         timeout=60) -> str:
+    """The reference's own renderer (src/Visualisation.cpp:11-129, built by
+    `make ref` as _ref/visual_emu) on gap-list files: returns its stdout.  Each
+    gap file gets one terminating record {-1, 0} appended first: the renderer
+    reads its gap lists without an end check (Visualisation.cpp:68,88)."""
+    import tempfile
+    if not os.path.exists(VISUAL_PATH):
+        raise FileNotFoundError(VISUAL_PATH)
+    td = tempfile.mkdtemp()
+    paths = []
+    for k, (seq, gp) in enumerate(((first, first_gaps), (second, second_gaps))):
+        sp = os.path.join(td, f"seq{k}.bin")
+        with open(sp, "wb") as f:
+            f.write(seq)
+        g = os.path.join(td, f"gaps{k}.bin")
+        with open(gp, "rb") as src, open(g, "wb") as dst:
+            dst.write(src.read())
+            dst.write(struct.pack("<ii", -1, 0))
+        paths += [sp, g]
+    p = subprocess.run([VISUAL_PATH, paths[0], paths[2], paths[1], paths[3], str(start[0]), str(start[1]),
+                        str(end[0]), str(end[1])], capture_output=True, timeout=timeout)
+    if p.returncode != 0:
+        raise RuntimeError(p.stderr.decode(errors="replace"))
+    return p.stdout.decode("latin-1")

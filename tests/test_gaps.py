@@ -145,3 +145,44 @@ def test_gap_lists_round_trip_property():
         assert _visual_output(rows, cols, g1, g2, (sr, sc), (er, ec)) == _render_ops(rows, cols, ops, sr, sc)
 
     check()
+
+
+def _cli_block_text(blocks):
+    """The CLI's alignment block as printed (cli.cpp render_alignment)."""
+    out = "\n\tVisual representation of the alignment:\n\n"
+    for l0, l1, l2 in blocks:
+        out += f"\t\t{l0}\n\t\t{l1}\n\t\t{l2}\n\n"
+    return out
+
+
+@pytest.mark.skipif(not os.path.exists(O.VISUAL_PATH), reason="reference renderer not built (make -C oracle ref)")
+@pytest.mark.parametrize("seed", range(8))
+def test_reference_renderer_prints_the_cli_block(tmp_path, seed):
+    """The gap-list files the library writes, rendered by the reference's own
+    visualOutput (src/Visualisation.cpp:11-129, CPU build), print exactly the
+    block the CLI renders from the operation string, byte for byte."""
+    rng = random.Random(300 + seed)
+    sc = (1, -3, -5, -2) if seed % 2 else (2, -3, -5, -2)
+    rows, cols, al = _alignment(rng, rng.randint(60, 900), sc)
+    f1, f2 = os.path.join(tmp_path, "first.gaps"), os.path.join(tmp_path, "second.gaps")
+    swb200.write_gap_lists(al, f1, f2)
+    got = O.run_reference_visual(rows, cols, f1, f2, (al.start_row, al.start_col), (al.end_row, al.end_col))
+    assert got == _cli_block_text(_render_ops(rows, cols, al.ops, al.start_row, al.start_col))
+
+
+@pytest.mark.skipif(not os.path.exists(O.VISUAL_PATH), reason="reference renderer not built (make -C oracle ref)")
+def test_reference_renderer_on_gap_runs_at_block_edges(tmp_path):
+    """Gap runs that start, end or straddle the 50-column block boundary, and no gaps at all."""
+    rng = random.Random(9)
+    for ops in ["M" * 49 + "I" * 3 + "M" * 10, "M" * 50 + "D" * 50 + "M", "M" * 120,
+                "M" + "I" * 49 + "M" + "D" * 51 + "M" * 3, "MIMDMIMDM" * 20]:
+        sr, scol = rng.randint(0, 9), rng.randint(0, 9)
+        rows = bytes(rng.choice(b"ACGT") for _ in range(sr + ops.count("M") + ops.count("D") + 3))
+        cols = bytes(rng.choice(b"ACGT") for _ in range(scol + ops.count("M") + ops.count("I") + 3))
+        al = types.SimpleNamespace(ops=ops, start_row=sr, start_col=scol)
+        er = sr + ops.count("M") + ops.count("D") - 1
+        ec = scol + ops.count("M") + ops.count("I") - 1
+        f1, f2 = os.path.join(tmp_path, "first.gaps"), os.path.join(tmp_path, "second.gaps")
+        swb200.write_gap_lists(al, f1, f2)
+        got = O.run_reference_visual(rows, cols, f1, f2, (sr, scol), (er, ec))
+        assert got == _cli_block_text(_render_ops(rows, cols, ops, sr, scol)), ops

@@ -169,3 +169,30 @@ def test_448_row_blocks(gpu_ctx, monkeypatch):
     a = a.replace(b"A", b"N", 40)
     r = _check(gpu_ctx, a, b, (2, -3, -5, -2))
     assert r.special_interval == 448
+
+
+@pytest.mark.skipif(not os.path.exists(O.VISUAL_PATH), reason="reference renderer not built (make -C oracle ref)")
+@pytest.mark.parametrize("fixture", [("1/A00142.fna.gz", "1/A00145.fna.gz", ("5", "-5", "-5", "-5")),
+                                     ("0/seq3.fna.gz", "0/seq4.fna.gz", ("1", "-3", "-5", "-2"))])
+def test_cli_block_equals_the_reference_renderer(tmp_path, fixture):
+    """The SWalign CLI's alignment block, and the reference's own visualOutput
+    (src/Visualisation.cpp:11-129, CPU build) run on the gap-list files the same
+    CLI run wrote (SWB_GAP_LISTS), are the same text byte for byte."""
+    import gzip
+    fa, fb, sc = fixture
+    pa, pb = tmp_path / "a.fna", tmp_path / "b.fna"
+    pa.write_bytes(gzip.open(os.path.join(GOLDEN, "seqs", fa)).read())
+    pb.write_bytes(gzip.open(os.path.join(GOLDEN, "seqs", fb)).read())
+    prefix = str(tmp_path / "gaps")
+    env = dict(os.environ, SWB_GAP_LISTS=prefix)
+    p = subprocess.run([swb200.CLI_PATH, str(pa), str(pb), *sc], capture_output=True, text=True, env=env)
+    assert p.returncode == 0, p.stdout + p.stderr
+    out = p.stdout
+    k = out.index("\n\tVisual representation of the alignment:\n\n")
+    block = out[k:]
+    xps = [line for line in out.splitlines() if line.startswith("\t>xPoint[")]
+    start = tuple(int(v) for v in xps[0].split("[")[2].split("]")[0].split(","))
+    end = tuple(int(v) for v in xps[-1].split("[")[2].split("]")[0].split(","))
+    rows, cols, _ = O.orient(load_fixture_fasta(fa), load_fixture_fasta(fb))
+    ref = O.run_reference_visual(rows, cols, prefix + ".first.bin", prefix + ".second.bin", start, end)
+    assert block == ref
