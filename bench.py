@@ -41,8 +41,9 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-mixed", action="store_true", help="skip the batched and serving measurements")
     p.add_argument("--batch-pairs", type=int, default=100_000, help="pairs of the batched workload")
-    p.add_argument("--serve-seconds", type=float, default=20.0, help="length of the Poisson serving run")
+    p.add_argument("--serve-seconds", type=float, default=60.0, help="length of the Poisson serving run")
     p.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
+    p.add_argument("--no-chromosome", action="store_true", help="skip the 10 Mbp chromosome-pair sub-record")
     return p.parse_args()
 
 
@@ -165,23 +166,26 @@ def cpu_model() -> str:
 
 
 def cpu_baseline(a: bytes, b: bytes, sc):
-    """The oracle's multithreaded CPU wavefront (same int32 recurrence) on a
-    bounded sample of the same pair: a band of rows against all columns, sized
-    for about 12 s on the host cores."""
+    """The oracle's fastest multithreaded CPU wavefront on this host (the AVX-512
+    one where the CPU has it, else the scalar one; same int32 recurrence and tie
+    rule) on a bounded sample of the same pair: a band of rows against all
+    columns, sized for about 12 s on the host cores."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_ctypes as O
     rows, cols, _ = O.orient(a, b)
     threads = os.cpu_count() or 1
     lo = len(rows) // 10
     probe_rows = max(1, min(len(rows) - lo, int(2e9 // len(cols))))
-    _, t = O.stage1_mt(rows[lo:lo + probe_rows], cols, O.scoring(*sc), threads=threads)
+    _, t, kind = O.stage1_fast(rows[lo:lo + probe_rows], cols, O.scoring(*sc), threads=threads)
     rate = probe_rows * len(cols) / max(t, 1e-6)
     nrows = max(1, min(len(rows) - lo, int(rate * 12.0 // len(cols))))
-    _, t = O.stage1_mt(rows[lo:lo + nrows], cols, O.scoring(*sc), threads=threads)
+    _, t, kind = O.stage1_fast(rows[lo:lo + nrows], cols, O.scoring(*sc), threads=threads)
     cells = nrows * len(cols)
+    impl = ("orc_stage1_simd: AVX-512 anti-diagonal strips of 16 rows" if kind == "avx512"
+            else "orc_stage1_mt: scalar blocked wavefront")
     return {"value": cells / t / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port", "cpu": cpu_model(),
             "sample": f"rows {lo}..{lo + nrows} of the rows sequence x all {len(cols)} columns "
-                      f"({cells:.3e} cells, {t:.1f} s), score + end cell"}
+                      f"({cells:.3e} cells, {t:.1f} s), score + end cell; {impl}"}
 
 
 def reference_arm(args):
@@ -234,6 +238,50 @@ def percentile(xs, q):
         return None
     k = min(len(xs) - 1, max(0, int(round(q / 100.0 * (len(xs) - 1)))))
     return xs[k]
+
+
+def chromosome_metrics(args, device, peak_cells_per_s):
+    """The chromosome-scale pair (two ~10 Mbp sequences, about 10^14 cells, special
+    rows and columns within a 40 GB budget): one warm-up and one timed full
+    alignment with the sequences resident in HBM, CUDA events on the library's
+    stream, clocks sampled during the timed step; checked against the oracle's
+    committed full-matrix golden when it exists."""
+    import torch
+    import swb200
+    a, b, sc_t, desc = workload("chromosome")
+    rows_b, cols_b = (a, b) if len(a) >= len(b) else (b, a)
+    m, n = len(rows_b), len(cols_b)
+    stream = torch.cuda.current_stream()
+    ctx = swb200.Context(device=device, cuda_stream=stream.cuda_stream, hbm_budget_bytes=40_000_000_000)
+    d_rows = torch.frombuffer(bytearray(rows_b), dtype=torch.uint8).cuda()
+    d_cols = torch.frombuffer(bytearray(cols_b), dtype=torch.uint8).cuda()
+    sc = swb200.scoring(*sc_t)
+    ctx.align_device(d_rows.data_ptr(), m, d_cols.data_ptr(), n, sc, 0)  # warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device) as clk:
+        e0.record(stream)
+        r = ctx.align_device(d_rows.data_ptr(), m, d_cols.data_ptr(), n, sc, 0)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ctx.close()
+    del d_rows, d_cols
+    torch.cuda.empty_cache()
+    golden = None
+    gpath = os.path.join(ROOT, "tests", "golden", "chromosome_golden.json")
+    if os.path.exists(gpath):
+        g = json.load(open(gpath))["reference"]
+        golden = (r.score, r.end_row, r.end_col) == (g["score"], g["end_row"], g["end_col"])
+    achieved = m * n / (r.stage1_ms * 1e-3) / 1e9
+    return {"workload": desc, "rows": m, "cols": n, "score": r.score, "end": [r.end_row + 1, r.end_col + 1],
+            "oracle_golden_match": golden, "gcups": m * n / (ms * 1e-3) / 1e9, "ms": ms,
+            "stage1_ms": r.stage1_ms, "stage2_ms": r.stage2_ms, "special_interval": r.special_interval,
+            "special_bytes": r.special_bytes, "alignment_ops": len(r.ops),
+            "roofline": {"achieved": achieved, "peak": peak_cells_per_s / 1e9, "unit": "GCUPS",
+                         "frac": achieved * 1e9 / peak_cells_per_s, "kernel": "stage1_kernel (scoring wavefront)"},
+            "timing": "1 warm-up + 1 timed full alignment (stage 1 + special rows + GPU traceback)",
+            "clocks": clk.summary()}
 
 
 def batched_metrics(args, device):
@@ -472,11 +520,15 @@ def main():
             dist.destroy_process_group()
         return
     cpu = None if args.no_cpu_baseline else cpu_baseline(a, b, sc_t)
-    mixed_batched = mixed_serving = None
+    mixed_batched = mixed_serving = chrom = None
+    ctx.close()
+    del d_rows, d_cols, flush
+    torch.cuda.empty_cache()
     if not args.no_mixed:
-        ctx.close()
         mixed_batched = batched_metrics(args, local)
         mixed_serving = None if args.no_serving else serving_metrics(args, local)
+    if not args.no_chromosome and args.workload == "long":
+        chrom = chromosome_metrics(args, local, peak_cells["cells_per_s"])
     d2h = 64 + first.n_ops + 24 * len(first.xpoints)
     line = {
         "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
@@ -500,6 +552,7 @@ def main():
         "gpu_launches": launches,
         "batched": mixed_batched,
         "serving": mixed_serving,
+        "chromosome": chrom,
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
