@@ -167,8 +167,12 @@ int swb_special_row_copy(swb_ctx *ctx, int64_t idx, int32_t *out, int64_t cols, 
  * 16.1 MiB per device that loads it, held until exit).  Limits: cols <=
  * SWB_NOALLOC_MAX_COLS, rows <= SWB_NOALLOC_MAX_ROWS, else SWB_EUNSUPPORTED.
  * The first call on a device looks up the array's device address; make it
- * before any stream capture.  Calls on one device that overlap on the GPU race
- * on the shared array.  `cuda_stream` is a cudaStream_t cast to an integer
+ * before any stream capture.  That first call also loads the array's module, which
+ * commits its memory and can fail with SWB_ECUDA (out of memory): callers that must
+ * not fail later make it at start-up, where a call with rows = cols = 0 does only
+ * this set-up.  The address is kept for the process: after a cudaDeviceReset of
+ * the device it is stale, so do not call this entry point on a device that was
+ * reset.  Calls on one device that overlap on the GPU race on the shared array.  `cuda_stream` is a cudaStream_t cast to an integer
  * (0 = legacy default stream); the call returns after the result is on the host.
  * Score-only (no traceback).  Error text: swb_noalloc_last_error(). */
 #define SWB_NOALLOC_MAX_COLS (1 << 20)

@@ -77,7 +77,6 @@ extern "C" int swb_score_pair_noalloc(int32_t device, const void *d_rows, int64_
     out->score = 0;
     out->end_row = 0;
     out->end_col = 0;
-    if (rows == 0 || cols == 0) return SWB_OK;
 
     int prev = -1;
     cudaGetDevice(&prev);
@@ -101,6 +100,8 @@ extern "C" int swb_score_pair_noalloc(int32_t device, const void *d_rows, int64_
         }
         base = (unsigned char *)g_scratch_addr[device];
     }
+    // an empty pair scores 0 at (0, 0); such a call does only the set-up above
+    if (rows == 0 || cols == 0) return SWB_OK;
     int sms = 0;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
         return noalloc_fail(SWB_ECUDA, cudaGetErrorString(e));

@@ -579,7 +579,13 @@ __global__ void __launch_bounds__(32) corridor_walk_kernel(WalkArgs a, const uin
         walk(a, R0, C0, SmemDir{dtile}, &sg, S);
         __syncwarp();
     }
-    if (in_flight) bar_wait(bar, phase & 1);  // a copy that outlived its wait: let it land (bounded)
+    // A copy still in flight after its wait ran out writes this CTA's shared
+    // memory, so the warp waits for it once more before the CTA exits.  It reads
+    // at most kBlockWords words of this GPU's own memory and lands in
+    // microseconds; every wait of the library is bounded (here about 1 s), and a
+    // copy that has not landed after two bounds means the device is failing: the
+    // error stays set for the host.
+    if (in_flight && !__all_sync(0xffffffffu, bar_wait(bar, phase & 1)) && lane == 0) S[kStErr] = 1;
     __syncwarp();
     if (lane < kStN) a.st[lane] = S[lane];
 }

@@ -71,3 +71,44 @@ def test_noalloc_refuses_sizes_beyond_its_scratch():
     rc = fn(0, C.c_void_p(1), too_many_cols, C.c_void_p(1), too_many_cols, C.byref(sc), 0, 0, C.byref(out))
     assert rc == swb200.SWB_EUNSUPPORTED
     assert b"SWB_NOALLOC_MAX" in err()
+
+
+def _compare_with_pair_path(pairs, flags=0):
+    import torch
+    fn, err = _noalloc()
+    sc = swb200.scoring(1, -3, -5, -2)
+    stream = torch.cuda.current_stream().cuda_stream
+    with swb200.Context(device=0) as ctx:
+        for r, c in pairs:
+            tr = torch.frombuffer(bytearray(r), dtype=torch.uint8).cuda()
+            tc = torch.frombuffer(bytearray(c), dtype=torch.uint8).cuda()
+            out = Score()
+            rc = fn(0, tr.data_ptr(), len(r), tc.data_ptr(), len(c), C.byref(sc), flags, stream, C.byref(out))
+            assert rc == swb200.SWB_OK, err()
+            ref = ctx.align_device(tr.data_ptr(), len(r), tc.data_ptr(), len(c), sc,
+                                   swb200.FLAG_SCORE_ONLY | flags)
+            assert (out.score, out.end_row, out.end_col) == (ref.score, ref.end_row, ref.end_col), (len(r), len(c))
+
+
+def test_noalloc_at_its_limits_and_with_the_rowmajor_tie():
+    """More strips than the scratch holds warps for (the grid is capped), the
+    widest pair the hand-off row allows (cols = SWB_NOALLOC_MAX_COLS), and the
+    row-major tie rule on a pair of all-equal maxima."""
+    rng = random.Random(11)
+    tall = bytes(rng.choice(b"ACGT") for _ in range(2_200_000))
+    tall_cols = tall[1_000_000:1_000_700]
+    wide = bytes(rng.choice(b"ACGT") for _ in range(1 << 20))
+    wide_cols = bytes(c if rng.random() > 0.05 else rng.choice(b"ACGT") for c in wide)
+    _compare_with_pair_path([(tall, tall_cols), (wide, wide_cols)])
+    _compare_with_pair_path([(b"A" * 3000, b"A" * 900)], swb200.FLAG_TIE_ROWMAJOR)
+
+
+def test_noalloc_set_up_call_with_empty_pair():
+    """rows = cols = 0 does only the per-device set-up and scores 0 at (0, 0)."""
+    fn, err = _noalloc()
+    sc = swb200.scoring(1, -3, -5, -2)
+    out = Score()
+    out.score = -1
+    rc = fn(0, None, 0, None, 0, C.byref(sc), 0, 0, C.byref(out))
+    assert rc == swb200.SWB_OK, err()
+    assert (out.score, out.end_row, out.end_col) == (0, 0, 0)
