@@ -158,6 +158,39 @@ int swb_reference_geometry(int64_t rows, int64_t cols, int32_t *G, int32_t *T, i
  * (src/Builders.cpp:41-61, read back at src/Crosspointer.cpp:94-102). */
 int swb_special_row_copy(swb_ctx *ctx, int64_t idx, int32_t *out, int64_t cols, int64_t *interval);
 
+/* One block of a pair split into blocks: the step of the multi-GPU column-chunk
+ * chain (swb200/chain.py), where GPU g owns a range of columns, walks it in
+ * blocks of rows and passes its right border to GPU g+1.  The reference runs
+ * one pair on one GPU (src/main.cu:125-126) and has no counterpart; this is the
+ * row recurrence of src/FindAlignment.cuh:54-56 over a sub-rectangle whose
+ * boundaries come from its neighbours instead of the zeroed buffers of
+ * src/SWutils.cpp:144-168.
+ *   block    rows [row_origin, +rows) x cols [col_origin, +cols) of a full_rows x
+ *            full_cols matrix (rows = the longer sequence); d_rows / d_cols are
+ *            the block's own bytes (device memory)
+ *   d_top    (H, F) int32 pairs of row row_origin - 1 over the block's columns,
+ *            or NULL at the matrix's top edge (zeros)
+ *   d_left   (H, E) int32 pairs of column col_origin - 1 over the block's rows,
+ *            or NULL at the left edge (zeros); corner = H[row_origin-1][col_origin-1]
+ *   d_bottom receives (H, F) of the block's last row (cols pairs), or NULL; needs
+ *            rows to be a multiple of 512
+ *   d_right  receives (H, E) of the block's last column (rows pairs), or NULL
+ * The best cell comes back in whole-matrix coordinates with its tie key: over
+ * all blocks the highest score, then the smallest key, is the pair's result
+ * (row, col = -1 and key = ~0 when no cell of the block is positive).  flags:
+ * SWB_FLAG_TIE_ROWMAJOR.  Runs on the context's stream and returns when the
+ * outputs are written. */
+typedef struct {
+    int32_t  score;
+    int64_t  row, col;
+    uint64_t key;
+    double   stage1_ms;
+} swb_block_best;
+int swb_score_block_device(swb_ctx *ctx, const void *d_rows, int64_t rows, const void *d_cols, int64_t cols,
+                           const int32_t *d_top, const int32_t *d_left, int32_t corner, int64_t row_origin,
+                           int64_t col_origin, int64_t full_rows, int64_t full_cols, const swb_scoring *sc,
+                           uint32_t flags, int32_t *d_bottom, int32_t *d_right, swb_block_best *out);
+
 /* Score and end cell of one pair, for callers that cannot allocate device
  * memory.  No counterpart in the reference (its stage 1 allocates its buffers
  * with cudaMalloc, src/SWutils.cpp:144-168).  Callers inside another framework's

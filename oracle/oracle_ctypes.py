@@ -76,6 +76,10 @@ def lib():
         L.orc_anchored_score.argtypes = [u8p, C.c_int64, u8p, C.c_int64, C.POINTER(Scoring),
                                          C.c_int64, C.c_int64, C.c_int64, C.c_int64]
         L.orc_anchored_score.restype = C.c_int64
+        L.orc_block.argtypes = [u8p, C.c_int64, u8p, C.c_int64, C.POINTER(Scoring), C.c_void_p, C.c_void_p,
+                                C.c_int32, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_void_p,
+                                C.c_void_p, C.POINTER(End), C.POINTER(C.c_uint64)]
+        L.orc_block.restype = C.c_int
         _lib = L
     return _lib
 
@@ -207,6 +211,25 @@ def score_ops(rows: bytes, cols: bytes, sc: Scoring, sr: int, scol: int, ops: st
 def anchored_score(rows: bytes, cols: bytes, sc: Scoring, sr: int, scol: int, er: int, ec: int) -> int:
     """Best score of an alignment from the diagonal cell (sr, scol) to (er, ec)."""
     return lib().orc_anchored_score(rows, len(rows), cols, len(cols), C.byref(sc), sr, scol, er, ec)
+
+
+def block(rows: bytes, cols: bytes, sc: Scoring, top, left, corner: int, r0: int, c0: int,
+          full_m: int, full_n: int, tie=TIE_REFERENCE):
+    """One block of a chain (orc_block): returns (bottom, right, Stage1 best, key);
+    top / left / bottom / right are int32 numpy arrays of shape (len, 2) or None."""
+    import numpy as np
+    m, n = len(rows), len(cols)
+    bottom = np.zeros((n, 2), dtype=np.int32)
+    right = np.zeros((m, 2), dtype=np.int32)
+    t = None if top is None else np.ascontiguousarray(top, dtype=np.int32)
+    lf = None if left is None else np.ascontiguousarray(left, dtype=np.int32)
+    e, key = End(), C.c_uint64(0)
+    rc = lib().orc_block(rows, m, cols, n, C.byref(sc), None if t is None else t.ctypes.data,
+                         None if lf is None else lf.ctypes.data, corner, r0, c0, full_m, full_n, tie,
+                         bottom.ctypes.data, right.ctypes.data, C.byref(e), C.byref(key))
+    if rc != 0:
+        raise RuntimeError(f"orc_block failed: {rc}")
+    return bottom, right, Stage1(e.score, e.row, e.col), key.value
 
 
 def crosspoints(ops: str, sr: int, scol: int, interval: int):

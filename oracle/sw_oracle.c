@@ -535,3 +535,55 @@ int64_t orc_anchored_score(const uint8_t *a, int64_t m, const uint8_t *b, int64_
     free(H); free(F);
     return res;
 }
+
+/* ------------------------------------------------------- one block of a chain */
+
+int orc_block(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n, const orc_scoring *sc,
+              const int32_t *top, const int32_t *left, int32_t corner,
+              int64_t r0, int64_t c0, int64_t full_m, int64_t full_n, int tie,
+              int32_t *bottom, int32_t *right, orc_end *best, uint64_t *bestkey) {
+    if (m <= 0 || n <= 0 || r0 < 0 || c0 < 0 || r0 + m > full_m || c0 + n > full_n) return -2;
+    orc_geom g;
+    if (orc_geometry(full_m, full_n, &g) != 0) tie = ORC_TIE_ROWMAJOR;
+    const int32_t ext = sc->gap_extend, open = sc->gap_open;
+    int32_t *H = malloc(sizeof(int32_t) * (size_t)n), *F = malloc(sizeof(int32_t) * (size_t)n);
+    if (!H || !F) { free(H); free(F); return -3; }
+    for (int64_t c = 0; c < n; ++c) {
+        H[c] = top ? top[2 * c] : 0;
+        F[c] = top ? top[2 * c + 1] : 0;
+    }
+    int32_t bs = 0;
+    uint64_t bk = ~0ULL;
+    int64_t br = 0, bc = 0;
+    int32_t hd_row = corner;                      /* H[r-1][c0-1] for the current row */
+    for (int64_t r = 0; r < m; ++r) {
+        int32_t hl = left ? left[2 * r] : 0, el = left ? left[2 * r + 1] : 0;
+        int32_t hd = hd_row;
+        hd_row = hl;
+        const uint8_t ar = a[r];
+        for (int64_t c = 0; c < n; ++c) {
+            const int32_t f = imax(F[c] + ext, H[c] + open);
+            const int32_t e = imax(el + ext, hl + open);
+            const int32_t s = (ar == b[c]) ? sc->match : sc->mismatch;
+            const int32_t h = imax(imax(0, e), imax(f, hd + s));
+            hd = H[c];
+            H[c] = h;
+            F[c] = f;
+            hl = h;
+            el = e;
+            if (h >= bs && h > 0) {
+                const uint64_t key = orc_tie_key(&g, tie, r0 + r, c0 + c);
+                if (h > bs || key < bk) { bs = h; bk = key; br = r0 + r; bc = c0 + c; }
+            }
+        }
+        if (right) { right[2 * r] = hl; right[2 * r + 1] = el; }
+    }
+    if (bottom)
+        for (int64_t c = 0; c < n; ++c) { bottom[2 * c] = H[c]; bottom[2 * c + 1] = F[c]; }
+    best->score = bs;
+    best->row = bs > 0 ? br : 0;
+    best->col = bs > 0 ? bc : 0;
+    *bestkey = bs > 0 ? bk : ~0ULL;
+    free(H); free(F);
+    return 0;
+}

@@ -104,6 +104,20 @@ int64_t orc_score_ops(const uint8_t *a, const uint8_t *b, const orc_scoring *sc,
 int64_t orc_anchored_score(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n,
                            const orc_scoring *sc, int64_t sr, int64_t sc_, int64_t er, int64_t ec);
 
+/* One block of a pair split into blocks (the multi-GPU column-chunk chain):
+ * rows [r0, r0+m) x cols [c0, c0+n) of a full_m x full_n matrix (a, b point at
+ * the block's own bytes), given top[2n] = (H, F) of row r0-1 over the block's
+ * columns and left[2m] = (H, E) of column c0-1 over its rows (NULL: the matrix
+ * edge, zeros) and corner = H[r0-1][c0-1].  Writes bottom[2n] = (H, F) of its
+ * last row and right[2m] = (H, E) of its last column (either may be NULL), and
+ * its best cell in whole-matrix coordinates with its tie key (~0 when no cell
+ * is positive), so that the best over all blocks with the smallest key among
+ * equal scores is the whole matrix's result.  Returns 0, or -2 / -3. */
+int orc_block(const uint8_t *a, int64_t m, const uint8_t *b, int64_t n, const orc_scoring *sc,
+              const int32_t *top, const int32_t *left, int32_t corner,
+              int64_t r0, int64_t c0, int64_t full_m, int64_t full_n, int tie,
+              int32_t *bottom, int32_t *right, orc_end *best, uint64_t *bestkey);
+
 #ifdef __cplusplus
 }
 #endif

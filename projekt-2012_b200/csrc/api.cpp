@@ -270,9 +270,19 @@ int check_scoring(swb_ctx *c, const swb_scoring *sc, int64_t rows, int64_t cols)
 }
 
 // Runs stage 1 on device sequences already in the context's buffers.
+
+// One block of a pair split into blocks (swb_score_block_device): boundaries in,
+// boundaries out, tie keys over the whole matrix.
+struct BlockIo {
+    const int2 *top = nullptr, *left = nullptr;
+    int32_t corner = 0;
+    int64_t r0 = 0, c0 = 0, full_m = 0, full_n = 0;
+    int2 *bottom = nullptr, *right = nullptr;
+};
+
 int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_cols, int64_t n,
                const swb_scoring *sc, uint32_t flags, int64_t sr_interval_rows, int64_t sc_interval,
-               swb::BestRec *best_out, float *ms_out, int64_t *nsr_out) {
+               swb::BestRec *best_out, float *ms_out, int64_t *nsr_out, const BlockIo *blk = nullptr) {
     using namespace swb;
     cudaError_t e;
     // TAB mode when the column sequence has at most four distinct bytes and the
@@ -325,11 +335,21 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     a.wait_limit = c->wait_cycles;
     int32_t G = 0, T = 0;
     int64_t P1 = 0, P2 = 0;
-    const bool refok = reference_geometry(m, n, &G, &T, &P1, &P2);
+    const bool refok = blk ? reference_geometry(blk->full_m, blk->full_n, &G, &T, &P1, &P2)
+                           : reference_geometry(m, n, &G, &T, &P1, &P2);
     a.tie.mode = ((flags & SWB_FLAG_TIE_ROWMAJOR) || !refok) ? kTieRowMajor : kTieReference;
     a.tie.G = G;
     a.tie.T = T;
     a.tie.C = refok ? P2 / G : 1;
+    if (blk) {
+        a.top = blk->top;
+        a.left = blk->left;
+        a.corner = blk->corner;
+        a.r_origin = blk->r0;
+        a.c_origin = blk->c0;
+        a.bottom = blk->bottom;
+        a.right = blk->right;
+    }
 
     // rows per lane: an override, else the autotuner.  Strips must tile the
     // special-row spacing when special rows are kept; sr_interval_rows < 0 asks
@@ -338,7 +358,8 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
     const bool strip_rows = sr_interval_rows < 0;
     const bool stores = sr_interval_rows != 0 || sc_interval > 0;
     int R = 16;
-    if (const char *rv = std::getenv("SWB_STAGE1_R")) R = std::atoi(rv);  // override: 8, 14, 16 or 32
+    if (blk && blk->bottom) R = 16;  // the last row must be a strip bottom: 512-row strips
+    else if (const char *rv = std::getenv("SWB_STAGE1_R")) R = std::atoi(rv);  // override: 8, 14, 16 or 32
     else R = autotune_rows_per_lane(c, a, tab, stores, 16, strip_rows, sr_interval_rows > 0 ? sr_interval_rows : 0);
     if (strip_rows) {
         if (R != 14 && R != 16) R = 16;
@@ -514,6 +535,45 @@ extern "C" int swb_align_pair_device(swb_ctx *c, const void *d_rows, int64_t row
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
     return align_device(c, (const uint8_t *)d_rows, rows, (const uint8_t *)d_cols, cols, sc, flags, out, 0);
+}
+
+extern "C" int swb_score_block_device(swb_ctx *c, const void *d_rows, int64_t rows, const void *d_cols, int64_t cols,
+                                      const int32_t *d_top, const int32_t *d_left, int32_t corner, int64_t row_origin,
+                                      int64_t col_origin, int64_t full_rows, int64_t full_cols, const swb_scoring *sc,
+                                      uint32_t flags, int32_t *d_bottom, int32_t *d_right, swb_block_best *out) {
+    if (!c || !out || rows <= 0 || cols <= 0 || !d_rows || !d_cols || row_origin < 0 || col_origin < 0 ||
+        full_rows < full_cols || row_origin + rows > full_rows || col_origin + cols > full_cols)
+        return ctx_fail(c, SWB_EINVAL, "swb_score_block_device: bad arguments");
+    if (full_rows > (int64_t)INT32_MAX - 64)
+        return ctx_fail(c, SWB_EUNSUPPORTED, "sequence longer than 2^31 - 64");
+    if (d_bottom && rows % 512 != 0)
+        return ctx_fail(c, SWB_EINVAL, "swb_score_block_device: the bottom row needs rows to be a multiple of 512");
+    int rc = check_scoring(c, sc, full_rows, full_cols);
+    if (rc != SWB_OK) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    BlockIo io;
+    io.top = (const int2 *)d_top;
+    io.left = (const int2 *)d_left;
+    io.corner = corner;
+    io.r0 = row_origin;
+    io.c0 = col_origin;
+    io.full_m = full_rows;
+    io.full_n = full_cols;
+    io.bottom = (int2 *)d_bottom;
+    io.right = (int2 *)d_right;
+    swb::BestRec best{};
+    float ms = 0.f;
+    rc = run_stage1(c, (const uint8_t *)d_rows, rows, (const uint8_t *)d_cols, cols, sc,
+                    flags & SWB_FLAG_TIE_ROWMAJOR, 0, 0, &best, &ms, nullptr, &io);
+    if (rc != SWB_OK) return rc;
+    const bool any = best.valid && best.ho - sc->gap_open > 0;
+    out->score = any ? best.ho - sc->gap_open : 0;
+    out->row = any ? row_origin + best.row : -1;
+    out->col = any ? col_origin + best.col : -1;
+    out->key = any ? best.key : ~0ULL;
+    out->stage1_ms = ms;
+    return SWB_OK;
 }
 
 extern "C" int swb_align_pair(swb_ctx *c, const uint8_t *a, int64_t la, const uint8_t *b, int64_t lb,

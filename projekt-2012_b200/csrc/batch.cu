@@ -75,6 +75,8 @@ struct PairView : S {
     TieGeom tie;
     int64_t wait_limit;
     static constexpr int32_t withhold = 0;
+    static constexpr int2 *bottom = nullptr;
+    static constexpr int2 *right = nullptr;
     static constexpr int64_t r_origin = 0;
     static constexpr int64_t c_origin = 0;
     static constexpr int64_t *trace = nullptr;

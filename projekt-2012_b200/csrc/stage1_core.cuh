@@ -119,6 +119,7 @@ struct StripCtx {
     int32_t n;
     bool sr;          // this strip's bottom row is a special row
     bool below;       // a strip below this one reads its bottom row from hbuf
+    bool last_row;    // this strip's bottom row is the rectangle's last row, kept in a.bottom
     int64_t sr_off;   // srows offset of that row
 };
 
@@ -283,12 +284,13 @@ template <class A>
 __device__ __forceinline__ void flush(const A &a, const int4 *stage, int lane, const StripCtx &sc, int32_t n,
                                       int32_t k) {
     __syncwarp();
-    if (lane < kCH && (sc.below || sc.sr)) {
+    if (lane < kCH && (sc.below || sc.sr || sc.last_row)) {
         const int32_t c = k - kCH - 31 + lane;
         if (c >= 0 && c < n) {
             const int4 v = stage[c & (kStage - 1)];
             if (sc.below) st_ll(a.hbuf + c, v.x, v.y, sc.strip);
             if (sc.sr) a.srows[sc.sr_off + c] = make_int2(v.x - a.open, v.z);
+            if (sc.last_row) a.bottom[c] = make_int2(v.x - a.open, v.z);
         }
     }
 }
@@ -328,6 +330,7 @@ __device__ bool run_strip(const A &a, int4 *ring, int4 *stage, int lane, int32_t
     sc.strip = s;
     sc.n = (int32_t)a.n;
     sc.below = (int64_t)(s + 1) * H < a.m && !(a.withhold && s == 0);
+    sc.last_row = a.bottom != nullptr && (int64_t)(s + 1) * H == a.m;
     sc.sr = a.srows != nullptr && ((int64_t)(s + 1) % a.sr_every) == 0 && (int64_t)(s + 1) * H <= a.m;
     sc.sr_off = sc.sr ? ((int64_t)(s + 1) / a.sr_every - 1) * a.n : 0;
     L.bho = bho;
@@ -427,6 +430,12 @@ __device__ bool run_strip(const A &a, int4 *ring, int4 *stage, int lane, int32_t
     // the columns staged since the last refill
     flush(a, stage, lane, sc, n, ((kEnd + kCH - 1) / kCH) * kCH);
     __syncwarp();
+    if (a.right != nullptr) {
+        // after its last column a lane's registers hold H + open and E of column n - 1
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+            if (sc.row0 + i < a.m) a.right[sc.row0 + i] = make_int2(L.HO[i] - a.open, L.E[i]);
+    }
     bho = L.bho;
     return true;
 }

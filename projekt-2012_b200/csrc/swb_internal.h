@@ -65,6 +65,8 @@ struct Stage1Args {
     TieGeom tie;
     int64_t wait_limit;    // bound of each wait for the strip above, in SM clock cycles; 0 = kWaitLimitCycles
     int32_t withhold;      // test hook: strip 0 writes no hand-off entries (SWB_FLAG_TEST_WITHHOLD)
+    int2 *bottom;          // optional: (H, F) of the last row, n entries (m a multiple of the strip height)
+    int2 *right;           // optional: (H, E) of the last column, m entries
 };
 
 // Geometry of the reference's launch (src/SWutils.cpp:233-253) and padding

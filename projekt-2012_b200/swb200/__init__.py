@@ -80,6 +80,11 @@ class ServerOptions(C.Structure):
                 ("max_batch", C.c_int32), ("reserve_sms", C.c_int32), ("flags", C.c_uint32)]
 
 
+class BlockBest(C.Structure):
+    _fields_ = [("score", C.c_int32), ("row", C.c_int64), ("col", C.c_int64), ("key", C.c_uint64),
+                ("stage1_ms", C.c_double)]
+
+
 class RequestInfo(C.Structure):
     _fields_ = [("queued_ms", C.c_double), ("run_ms", C.c_double), ("total_ms", C.c_double),
                 ("lane", C.c_int32), ("batch_size", C.c_int32)]
@@ -128,6 +133,11 @@ def lib():
         L.swb_align_pair_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
                                             C.POINTER(Scoring), C.c_uint32, C.POINTER(Result)]
         L.swb_align_pair_device.restype = C.c_int
+        L.swb_score_block_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p,
+                                             C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_int64, C.c_int64,
+                                             C.POINTER(Scoring), C.c_uint32, C.c_void_p, C.c_void_p,
+                                             C.POINTER(BlockBest)]
+        L.swb_score_block_device.restype = C.c_int
         L.swb_result_free.argtypes = [C.POINTER(Result)]
         L.swb_reference_geometry.argtypes = [C.c_int64, C.c_int64, C.POINTER(C.c_int32),
                                              C.POINTER(C.c_int32), C.POINTER(C.c_int64),

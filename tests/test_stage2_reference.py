@@ -95,7 +95,8 @@ def test_gpu_against_the_reference_stage2_sweep(gpu_ctx):
 def test_gpu_against_the_reference_stage2_on_real_fixtures(gpu_ctx):
     """seq3/seq4: the reference's list equals the GPU's; seq0/seq1: same start and
     end, the reference's search missed the crosspoint between them; A00142/A00145:
-    the reference printed the end cell only (its start search found nothing)."""
+    the reference printed the end cell only (its start search found nothing), with
+    its stage-1 score, which its left-boundary carry inflates at the same cell."""
     checked = 0
     for f in load_json("refemu_fixtures.json"):
         s2 = f.get("stage2", {})
@@ -104,8 +105,16 @@ def test_gpu_against_the_reference_stage2_on_real_fixtures(gpu_ctx):
         a, b = load_fixture_fasta(f["a"]), load_fixture_fasta(f["b"])
         ref = [tuple(x) for x in s2["xpoints"]]
         if len(ref) == 1:
+            # end cell only; the reference's own stage 1 scored it with its
+            # left-boundary carry (520 where textbook Gotoh gives 480 at the same cell)
+            rows, cols, _ = O.orient(a, b)
+            s = O.scoring(*f["scoring"])
+            c = O.stage1(rows, cols, s, O.SHIPPED_CARRY, O.TIE_REFERENCE)
+            assert ref[0][:3] == (c.row, c.col, c.score)
+            e = O.stage1(rows, cols, s, O.TEXTBOOK, O.TIE_REFERENCE)
             r = gpu_ctx.align(a, b, swb200.scoring(*f["scoring"]))
-            assert tuple(r.xpoints[-1]) == ref[0]
+            assert tuple(r.xpoints[-1]) == (e.row, e.col, e.score, 0)
+            assert (r.end_row, r.end_col) == ref[0][:2]
             checked += 1
             continue
         rel = relation(a, b, f["scoring"], ref)
