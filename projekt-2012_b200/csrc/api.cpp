@@ -505,7 +505,10 @@ int align_device(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_
             return swb::ctx_put((swb_ctx *)owner, dst, src, bytes);
         };
         int32_t launches = 0;
-        rc = tb::traceback(c->stream, c->sms, d_rows, m, d_cols, n, sc, plan, (const int2 *)c->srows.p,
+        // a capped context (the serving loop's long lane) sizes its stage-2 grids
+        // to the same share of the GPU as its stage 1 (4 scoring blocks per SM)
+        const int tb_sms = c->max_blocks > 0 ? std::max(1, std::min(c->sms, c->max_blocks / 4)) : c->sms;
+        rc = tb::traceback(c->stream, tb_sms, d_rows, m, d_cols, n, sc, plan, (const int2 *)c->srows.p,
                            (const int2 *)c->scols.p, out, scr, c->err, &launches);
         if (rc != SWB_OK) return ctx_fail(c, rc, "%s", c->err.c_str());
         out->kernel_launches += launches;

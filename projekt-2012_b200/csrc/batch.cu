@@ -128,10 +128,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs &g) {
             v.corner = (d.top && d.left) ? d.top[-1].x : 0;
         }
         Best b;
-        b.ho = g.open + 1;  // only H >= 1 is recorded
-        b.key = ~0ULL;
-        b.row = 0;
-        b.col = 0;
+        init_best(b, g.open);
         int32_t bho = b.ho;
         if (!run_strip<R, TAB, !std::is_same<S, NoStores>::value, false>(v, ring, stage, lane, u - d.unit0, &b, bho)) {
             if (lane == 0) {
@@ -140,6 +137,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs &g) {
             }
             break;
         }
+        key_best(&b, v.tie, v.r_origin, v.c_origin);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
             const int32_t oho = __shfl_xor_sync(0xffffffffu, b.ho, off);

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstddef>
 #include <chrono>
+#include <cstdio>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -174,6 +175,21 @@ bool graphs_enabled() {
     return !(v && v[0] == '0');
 }
 
+// Host phases of a batched call on stderr (options.verbose bit 0): the time
+// since the previous mark, in ms.
+struct PhaseLog {
+    bool on;
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    explicit PhaseLog(const swb_ctx *c) : on(c && (c->opts.verbose & 1)) {}
+    void mark(const char *what) {
+        if (!on) return;
+        const auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "swb batch: %-22s %9.3f ms\n", what,
+                     std::chrono::duration<double, std::milli>(now - t).count());
+        t = now;
+    }
+};
+
 size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 
 size_t pow2_at_least(size_t x) {
@@ -311,10 +327,12 @@ int graph_pass(swb_ctx *c, const uint8_t *h_seq, int64_t seq_bytes, const std::v
                const std::vector<int64_t> &order, const swb_scoring *sc, uint32_t flags, bool traced,
                swb_batch_result *out, GraphPass &gp) {
     cudaError_t e;
+    PhaseLog ph(c);
     const int R = traced ? kBatchR : batch_score_rows_per_lane();
     std::vector<int32_t> unit_pair;
     int64_t hb = 0, srn = 0, scn = 0, ops_total = 0, xp_total = 0;
     layout_units(info, order, flags, 32 * R, gp.bp, unit_pair, &hb);
+    ph.mark("graph: layout units");
     const int64_t np = (int64_t)gp.bp.size(), nu = (int64_t)unit_pair.size();
     const int kS = tb::state_slots();
     if (traced) {
@@ -434,7 +452,9 @@ int graph_pass(swb_ctx *c, const uint8_t *h_seq, int64_t seq_bytes, const std::v
         }
         tb::pack_walk_args(win.data(), np, g.walk_states, hin + in_walk);
     }
+    ph.mark("graph: descriptors");
     copy_parallel(hin + in_seq, h_seq, (size_t)seq_bytes);
+    ph.mark("graph: sequences staged");
     // size class: the smallest power of two >= the unit count (pairs <= units), up
     // to one that no longer shrinks any grid
     int size_class = 0;
@@ -455,6 +475,7 @@ int graph_pass(swb_ctx *c, const uint8_t *h_seq, int64_t seq_bytes, const std::v
         (e = cudaMemcpyAsync(hout, dout, out_bytes, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
         return ctx_cuda_fail(c, e, "batch graph replay");
+    ph.mark("graph: copies + replay");
     const int32_t *ctl = (const int32_t *)(hout + o_ctl);
     if (ctl[1] != 0) return ctx_fail(c, SWB_ETIMEOUT, "batch: a bounded wait between strips ran out");
     gp.tab = ctl[4] != 0;
@@ -482,6 +503,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
               int64_t npairs, const swb_scoring *sc, uint32_t flags, double trace_frac, swb_batch_result *out,
               bool stores_first) {
     const auto t0 = std::chrono::steady_clock::now();
+    PhaseLog ph(c);
     std::memset(out, 0, sizeof *out);
     if (!sc) return ctx_fail(c, SWB_EINVAL, "scoring is NULL");
     if (sc->match < 1 || sc->mismatch > -1 || sc->gap_open > -1 || sc->gap_extend > -1)
@@ -541,6 +563,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
     // partially traced batch launch their kernels directly
     const bool use_graph = h_seq != nullptr && !order.empty() && graphs_enabled();
     GraphPass gp;
+    ph.mark("orient + order");
     if (use_graph) {
         int rc = graph_pass(c, h_seq, seq_bytes, info, order, sc, flags, stores_first, out, gp);
         if (rc != SWB_OK) return rc;
@@ -648,6 +671,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
         out->items[i].start_col = out->items[i].end_col;
     }
     out->stage1_ms = ms1;
+    ph.mark("scoring pass");
 
     // traceback of the best-scoring pairs
     const int64_t ntrace =
@@ -671,6 +695,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
         out->n_traced = ntrace;
         // the layout whose special rows and columns the walker reads, per traced pair
         std::vector<BatchPair> bpw(tr.size());
+        ph.mark("select traced pairs");
         if (first_stores) {
             std::vector<int64_t> pos((size_t)npairs, -1);
             for (size_t k = 0; k < order.size(); ++k) pos[(size_t)order[k]] = (int64_t)k;
@@ -699,6 +724,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
                     return ctx_fail(c, SWB_ECUDA, "batch: store pass disagrees with the scoring pass");
             }
         }
+        ph.mark("store pass");
         if (!tr.empty()) {
             const int kS = tb::state_slots();
             // per traced pair: walker state, reversed ops / crosspoints and their capacities
@@ -793,6 +819,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
                     tXc[k] = win[k].xp_cap;
                 }
             }
+            ph.mark("walker");
             // gather: ops (end -> start on the device) and crosspoints
             int64_t tot_ops = 0, tot_xp = 0;
             for (size_t k = 0; k < tr.size(); ++k) {
@@ -845,6 +872,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
         out->stage2_ms = (use_graph && first_stores ? (double)gp.ms2 : 0.0) +
                          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
     }
+    ph.mark("results");
     out->kernel_launches = launches;
     out->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return SWB_OK;

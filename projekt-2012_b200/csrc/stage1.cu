@@ -60,10 +60,7 @@ __global__ void __launch_bounds__(kWarps * 32, (R <= 16 ? 4 : 2)) stage1_kernel(
     const int64_t B = gridDim.x;
 
     Best b;
-    b.ho = a.open + 1;  // only H >= 1 is recorded
-    b.key = ~0ULL;
-    b.row = 0;
-    b.col = 0;
+    init_best(b, a.open);
     int32_t bho = b.ho;
     bool failed = false;
     for (int64_t round = 0; !failed; ++round) {
@@ -85,6 +82,7 @@ __global__ void __launch_bounds__(kWarps * 32, (R <= 16 ? 4 : 2)) stage1_kernel(
         atomicCAS(&a.err[0], kErrNone, kErrTimeout);
         atomicExch(&a.err[1], 1);
     }
+    key_best(&b, a.tie, a.r_origin, a.c_origin);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         const int32_t oho = __shfl_xor_sync(0xffffffffu, b.ho, off);

@@ -72,28 +72,60 @@ __device__ __forceinline__ bool better(int32_t ho, uint64_t key, int32_t bho, ui
     return ho > bho || (ho == bho && key < bkey);
 }
 
+// A lane's best cell.  Its tie key is computed when first needed: along an
+// alignment path almost every new best is strictly better than the lane's
+// previous one and alone in its column, so no key is compared (evaluating the
+// reference key there, with its integer divisions, at every column the path
+// crosses made each strip's slow steps, and through the strip chain the whole
+// pass, about 13% slower on the 1 Mbp pair).
 struct Best {
     int32_t ho;
-    uint64_t key;
+    int32_t keyed;   // key holds the tie key of (row, col); else it is computed on demand
+    uint64_t key;    // ~0: no cell yet
     int64_t row, col;
 };
+
+__device__ __forceinline__ void init_best(Best &b, int32_t open) {
+    b.ho = open + 1;  // only H >= 1 is recorded
+    b.keyed = 1;
+    b.key = ~0ULL;
+    b.row = 0;
+    b.col = 0;
+}
+
+__device__ __forceinline__ void key_best(Best *b, const TieGeom tie, int64_t r_origin, int64_t c_origin) {
+    if (!b->keyed) {
+        b->key = tie_key(tie, r_origin + b->row, c_origin + b->col);
+        b->keyed = 1;
+    }
+}
 
 // Rows of `mask` hold the column maximum cm at column j: keep the smallest key.
 __device__ __forceinline__ int32_t slow_best(uint32_t mask, int32_t cm, const TieGeom tie, int64_t m, int64_t r_origin,
                                           int64_t c_origin, Best *b, int64_t row0, int32_t j, int32_t *gbest,
                                           int32_t open) {
     const int32_t before = b->ho;
-    while (mask) {
-        const int i = __ffs(mask) - 1;
-        mask &= mask - 1;
-        const int64_t r = row0 + i;
-        if (r >= m) break;
-        const uint64_t key = tie_key(tie, r_origin + r, c_origin + j);
-        if (better(cm, key, b->ho, b->key)) {
-            b->ho = cm;
-            b->key = key;
-            b->row = r;
-            b->col = j;
+    if (row0 + 32 > m) mask &= (m - row0 > 0) ? (uint32_t)((1ULL << (m - row0)) - 1ULL) : 0u;  // rows past the end
+    if (mask == 0) return b->ho;
+    if (cm > b->ho && (mask & (mask - 1)) == 0) {
+        // strictly better than anything this lane holds, and a single cell
+        b->ho = cm;
+        b->keyed = 0;
+        b->row = row0 + __ffs(mask) - 1;
+        b->col = j;
+    } else {
+        key_best(b, tie, r_origin, c_origin);
+        while (mask) {
+            const int i = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const int64_t r = row0 + i;
+            const uint64_t key = tie_key(tie, r_origin + r, c_origin + j);
+            if (better(cm, key, b->ho, b->key)) {
+                b->ho = cm;
+                b->key = key;
+                b->row = r;
+                b->col = j;
+            }
         }
     }
     if (b->ho > before) atomicMax(gbest, b->ho - open);
