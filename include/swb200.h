@@ -71,6 +71,12 @@ typedef struct {
  * returns SWB_ETIMEOUT with the context still usable.  Pairs of one strip (at
  * most 448 rows) have no wait and are unaffected. */
 #define SWB_FLAG_TEST_WITHHOLD 0x80000000u
+/* Test hook of swb_batch_align[_device]: the packed 16-bit scoring pass takes
+ * every pair, also those whose best score may not fit 16 bits; a pair that
+ * reaches the limit is detected and scored again in int32, so results do not
+ * change.  Without it only pairs whose score is bounded below the limit are
+ * packed. */
+#define SWB_FLAG_TEST_PACK_ANY 0x40000000u
 
 typedef struct {
     int32_t score;

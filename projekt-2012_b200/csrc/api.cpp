@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "ctx.h"
+#include "batch.h"
 #include "traceback.h"
 
 #define SWB_VERSION_STRING "swb200 0.1.0 (sm_100a)"
@@ -165,6 +166,7 @@ int swb_ctx_create(const swb_options *opts, swb_ctx **out) {
         (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess ||
         (e = cudaEventCreate(&c->ev2)) != cudaSuccess ||
         (e = swb::stage1_configure()) != cudaSuccess || (e = swb::batch_configure()) != cudaSuccess ||
+        (e = swb::batch16_configure()) != cudaSuccess ||
         (e = swb::tb::walker_configure()) != cudaSuccess) {
         int rc = ctx_cuda_fail(nullptr, e, "swb_ctx_create");
         // release what was created before the failure

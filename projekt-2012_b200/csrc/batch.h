@@ -55,6 +55,44 @@ struct BatchArgs {
     int64_t wait_limit;        // bound of each wait for the strip above, in SM clock cycles; 0 = default
 };
 
+// Two pairs scored side by side in packed 16-bit lanes (batch16.cu): half 0 is
+// pair a (low 16 bits of every lane register), half 1 pair b.  Both have the
+// same strip count; the packed rectangle is M = max(m) rows x N = max(n) columns.
+struct PackedPair {
+    int64_t row_off[2], col_off[2];  // byte offsets of each pair's rows / cols in the sequence buffer
+    int64_t hbuf_off;                // first of the N hand-off entries (packs of more than one strip)
+    int32_t m[2], n[2];              // m = n = 0: an empty half
+    int32_t M, N;
+    int32_t unit0, nstrips;          // units [unit0, unit0 + nstrips) of this launch
+    int32_t slot[2];                 // pbest / gbest / saturation slot of each half
+    TieGeom tie[2];
+};
+
+// Uniform arguments of one packed launch (TAB mode only: table words and row codes).
+struct Batch16Args {
+    const uint8_t *rcode;
+    const uint32_t *ctab;
+    uint32_t open2, ext2, gx2;  // gap_open, gap_extend, max of both in both halves
+    int32_t open;
+    uint32_t mm4;               // the table word of a column past a pair's end (a mismatch for every code)
+    int32_t sat_lim;            // a half's column maximum (H + open) at or above this flags its pair
+    const PackedPair *pairs;
+    const int32_t *unit_pair;   // work unit -> packed pair
+    int64_t nunits;
+    int4 *hbuf;
+    int32_t *gbest;             // per slot: best H seen so far
+    BestRec *ubest;             // per unit: two records (half 0, half 1)
+    int32_t *ctl;               // [0] unit counter, [1] error code, [2] abort flag
+    int32_t *sat;               // per slot: 1 when the pair reached the 16-bit limit
+    int64_t wait_limit;
+};
+
+constexpr int kBatch16R = 14;  // rows per lane of the packed kernel
+
+cudaError_t batch16_configure();
+cudaError_t batch16_launch(const Batch16Args &a, int sms, int max_blocks, int64_t npacked, BestRec *pbest,
+                           cudaStream_t st);
+
 // Rows per lane of the batched kernel's store passes (their strips are 512 rows,
 // the walker's block height); score-only passes may use 8 (256-row strips).
 constexpr int kBatchR = 16;

@@ -175,6 +175,145 @@ bool graphs_enabled() {
     return !(v && v[0] == '0');
 }
 
+// The packed 16-bit scoring pass (batch16.cu) serves score-only passes of
+// batches with at least this many pairs in the table (<= 4 letter) mode; the
+// smaller batches of the serving loop keep the replayed graph.
+constexpr int64_t kPackMinPairs = 2048;
+
+bool packing_enabled() {
+    const char *v = std::getenv("SWB_BATCH_PACK");
+    return !(v && v[0] == '0');
+}
+
+// Highest H + open a half of a packed lane may reach before its pair is scored
+// again in int32; a pair whose best score is bounded by match * n + 256 below
+// it is packed without that risk.
+constexpr int32_t kSatLimit = 32767 - 256;
+
+// The packed scoring pass over the positions `pos` of `order`: pairs sorted by
+// strip count and width and taken two at a time (a pair whose neighbour has
+// another strip count gets an empty partner).  Fills pbest[k] for every k in
+// pos and appends to `redo` the positions whose pair reached the 16-bit limit.
+int run_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &info,
+               const std::vector<int64_t> &order, std::vector<int64_t> pos, uint32_t flags,
+               std::vector<BestRec> &pbest, std::vector<int64_t> &redo, float *ms) {
+    cudaError_t e;
+    const int64_t H = 32LL * kBatch16R;
+    auto strips = [&](int64_t k) { return (info[(size_t)order[(size_t)k]].m + H - 1) / H; };
+    std::stable_sort(pos.begin(), pos.end(), [&](int64_t x, int64_t y) {
+        const int64_t sx = strips(x), sy = strips(y);
+        if (sx != sy) return sx > sy;
+        return info[(size_t)order[(size_t)x]].n > info[(size_t)order[(size_t)y]].n;
+    });
+    const int32_t dummy = (int32_t)order.size();  // slot of an empty half
+    std::vector<PackedPair> pp;
+    std::vector<int32_t> up;
+    int64_t units = 0, hb = 0;
+    for (size_t i = 0; i < pos.size();) {
+        const int64_t ka = pos[i];
+        const int64_t kb = (i + 1 < pos.size() && strips(pos[i + 1]) == strips(ka)) ? pos[i + 1] : -1;
+        i += kb >= 0 ? 2 : 1;
+        PackedPair d;
+        std::memset(&d, 0, sizeof d);
+        const int64_t ks[2] = {ka, kb};
+        for (int h = 0; h < 2; ++h) {
+            if (ks[h] < 0) {
+                d.slot[h] = dummy;
+                d.tie[h].mode = kTieRowMajor;
+                continue;
+            }
+            const PairInfo &p = info[(size_t)order[(size_t)ks[h]]];
+            d.row_off[h] = p.row_off;
+            d.col_off[h] = p.col_off;
+            d.m[h] = (int32_t)p.m;
+            d.n[h] = (int32_t)p.n;
+            d.slot[h] = (int32_t)ks[h];
+            int32_t G = 0, T = 0;
+            int64_t P1 = 0, P2 = 0;
+            const bool refok = reference_geometry(p.m, p.n, &G, &T, &P1, &P2);
+            d.tie[h].mode = ((flags & SWB_FLAG_TIE_ROWMAJOR) || !refok) ? kTieRowMajor : kTieReference;
+            d.tie[h].G = G;
+            d.tie[h].T = T;
+            d.tie[h].C = refok ? P2 / G : 1;
+        }
+        d.M = std::max(d.m[0], d.m[1]);
+        d.N = std::max(d.n[0], d.n[1]);
+        d.nstrips = (int32_t)((d.M + H - 1) / H);
+        d.unit0 = (int32_t)units;
+        if (d.nstrips > 1) {
+            d.hbuf_off = hb;
+            hb += d.N;
+        }
+        for (int32_t s = 0; s < d.nstrips; ++s) up.push_back((int32_t)pp.size());
+        units += d.nstrips;
+        pp.push_back(d);
+    }
+    const int64_t np = (int64_t)pp.size(), nslots = (int64_t)order.size() + 1;
+    const size_t pp_bytes = sizeof(PackedPair) * (size_t)np, up_bytes = sizeof(int32_t) * (size_t)units;
+    const size_t back = sizeof(BestRec) * (size_t)nslots + sizeof(int32_t) * (size_t)nslots + 64;
+    if ((e = c->b_pairs.ensure(pp_bytes)) != cudaSuccess || (e = c->b_units.ensure(up_bytes)) != cudaSuccess ||
+        (e = c->b_hbuf.ensure(sizeof(int4) * (size_t)std::max<int64_t>(1, hb))) != cudaSuccess ||
+        (e = c->b_gbest.ensure(sizeof(int32_t) * (size_t)nslots)) != cudaSuccess ||
+        (e = c->b_ubest.ensure(2 * sizeof(BestRec) * (size_t)std::max<int64_t>(1, units))) != cudaSuccess ||
+        (e = c->b_pbest.ensure(sizeof(BestRec) * (size_t)nslots)) != cudaSuccess ||
+        (e = c->b_sat.ensure(sizeof(int32_t) * (size_t)nslots)) != cudaSuccess ||
+        (e = c->b_ctl.ensure(4 * sizeof(int32_t))) != cudaSuccess ||
+        (e = c->h_stage.ensure(std::max(pp_bytes + up_bytes, back) + 64)) != cudaSuccess)
+        return ctx_cuda_fail(c, e, "packed batch buffers");
+    uint8_t *hs = (uint8_t *)c->h_stage.p;
+    std::memcpy(hs, pp.data(), pp_bytes);
+    std::memcpy(hs + pp_bytes, up.data(), up_bytes);
+    Batch16Args a{};
+    a.rcode = base.rcode;
+    a.ctab = base.ctab;
+    a.open = base.open;
+    a.open2 = (uint32_t)(uint16_t)(int16_t)base.open * 0x00010001u;
+    a.ext2 = (uint32_t)(uint16_t)(int16_t)base.ext * 0x00010001u;
+    a.gx2 = (uint32_t)(uint16_t)(int16_t)base.gx * 0x00010001u;
+    a.mm4 = base.tab_hi;
+    a.sat_lim = kSatLimit;
+    a.pairs = (const PackedPair *)c->b_pairs.p;
+    a.unit_pair = (const int32_t *)c->b_units.p;
+    a.nunits = units;
+    a.hbuf = (int4 *)c->b_hbuf.p;
+    a.gbest = (int32_t *)c->b_gbest.p;
+    a.ubest = (BestRec *)c->b_ubest.p;
+    a.ctl = (int32_t *)c->b_ctl.p;
+    a.sat = (int32_t *)c->b_sat.p;
+    a.wait_limit = c->wait_cycles;
+    if ((e = cudaMemcpyAsync(c->b_pairs.p, hs, pp_bytes, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(c->b_units.p, hs + pp_bytes, up_bytes, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+        (hb > 0 && (e = cudaMemsetAsync(a.hbuf, 0xFF, sizeof(int4) * (size_t)hb, c->stream)) != cudaSuccess) ||
+        (e = cudaMemsetAsync(a.gbest, 0, sizeof(int32_t) * (size_t)nslots, c->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(c->b_pbest.p, 0, sizeof(BestRec) * (size_t)nslots, c->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(a.sat, 0, sizeof(int32_t) * (size_t)nslots, c->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(a.ctl, 0, 4 * sizeof(int32_t), c->stream)) != cudaSuccess)
+        return ctx_cuda_fail(c, e, "packed batch set-up");
+    cudaEventRecord(c->ev0, c->stream);
+    if ((e = batch16_launch(a, c->sms, c->max_blocks, np, (BestRec *)c->b_pbest.p, c->stream)) != cudaSuccess)
+        return ctx_cuda_fail(c, e, "packed batch launch");
+    cudaEventRecord(c->ev1, c->stream);
+    BestRec *hb_best = (BestRec *)hs;
+    int32_t *hsat = (int32_t *)(hs + sizeof(BestRec) * (size_t)nslots);
+    int32_t *hctl = hsat + nslots;
+    if ((e = cudaMemcpyAsync(hb_best, c->b_pbest.p, sizeof(BestRec) * (size_t)nslots, cudaMemcpyDeviceToHost,
+                             c->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(hsat, a.sat, sizeof(int32_t) * (size_t)nslots, cudaMemcpyDeviceToHost, c->stream)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(hctl, a.ctl, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+        return ctx_cuda_fail(c, e, "packed batch");
+    if (hctl[1] != 0) return ctx_fail(c, SWB_ETIMEOUT, "batch: a bounded wait between strips ran out");
+    for (int64_t k : pos) {
+        if (hsat[k]) redo.push_back(k);
+        else pbest[(size_t)k] = hb_best[k];
+    }
+    float t = 0.f;
+    cudaEventElapsedTime(&t, c->ev0, c->ev1);
+    if (ms) *ms += t;
+    return SWB_OK;
+}
+
 // Host phases of a batched call on stderr (options.verbose bit 0): the time
 // since the previous mark, in ms.
 struct PhaseLog {
@@ -561,7 +700,12 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
     // host batches run as one replayed graph (sequences and descriptors in one
     // copy, results in one copy); device batches and the store pass of a
     // partially traced batch launch their kernels directly
-    const bool use_graph = h_seq != nullptr && !order.empty() && graphs_enabled();
+    // large score-only batches take the packed 16-bit pass (direct launches); the
+    // rest of host batches run as one replayed graph
+    const int32_t mt1 = sc->match - sc->gap_open, mm1 = sc->mismatch - sc->gap_open;
+    const bool pack_candidate = !stores_first && (int64_t)order.size() >= kPackMinPairs && packing_enabled() &&
+                                mt1 >= -128 && mt1 <= 127 && mm1 >= -128 && mm1 <= 127;
+    const bool use_graph = h_seq != nullptr && !order.empty() && graphs_enabled() && !pack_candidate;
     GraphPass gp;
     ph.mark("orient + order");
     if (use_graph) {
@@ -571,10 +715,18 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
 
     const uint8_t *d_seq = d_seq_in;
     if (h_seq && !use_graph) {
-        if ((e = c->b_seq.ensure((size_t)seq_bytes + 64)) != cudaSuccess) return ctx_cuda_fail(c, e, "batch sequences");
-        if ((e = ctx_put(c, c->b_seq.p, h_seq, (size_t)seq_bytes)) != cudaSuccess)
+        // through the context's pinned staging, copied in by several threads
+        if ((e = c->b_seq.ensure((size_t)seq_bytes + 64)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(c->stream)) != cudaSuccess ||
+            (e = c->h_io.ensure((size_t)std::max<int64_t>(1, seq_bytes))) != cudaSuccess)
+            return ctx_cuda_fail(c, e, "batch sequences");
+        copy_parallel((uint8_t *)c->h_io.p, h_seq, (size_t)seq_bytes);
+        if (seq_bytes > 0 &&
+            (e = cudaMemcpyAsync(c->b_seq.p, c->h_io.p, (size_t)seq_bytes, cudaMemcpyHostToDevice, c->stream)) !=
+                cudaSuccess)
             return ctx_cuda_fail(c, e, "copy batch sequences");
         d_seq = (const uint8_t *)c->b_seq.p;
+        ph.mark("sequences to the device");
     }
 
     BatchArgs base{};
@@ -641,10 +793,38 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
         bp = gp.bp;
         pbest = gp.pbest;
         ms1 = gp.ms1;
-    } else {
+    } else if (!(pack_candidate && tab)) {
         layout_units(info, order, flags, 32 * R1, bp, unit_pair, &hb);
     }
-    if (!order.empty() && !use_graph) {
+    if (!order.empty() && !use_graph && pack_candidate && tab) {
+        // pairs whose best score is bounded below the 16-bit limit run packed two
+        // per warp; the others, and any pair that reached the limit, in int32
+        std::vector<int64_t> ppos, rest;
+        for (size_t k = 0; k < order.size(); ++k) {
+            const PairInfo &p = info[(size_t)order[k]];
+            const bool fits = (int64_t)sc->match * p.n + 256 <= 32767 - 256;
+            if (fits || (flags & SWB_FLAG_TEST_PACK_ANY)) ppos.push_back((int64_t)k);
+            else rest.push_back((int64_t)k);
+        }
+        pbest.assign(order.size(), BestRec{});
+        int rc = run_packed(c, base, info, order, ppos, flags, pbest, rest, &ms1);
+        if (rc != SWB_OK) return rc;
+        launches += 2;
+        ph.mark("packed pass");
+        if (!rest.empty()) {
+            std::vector<int64_t> sub(rest.size());
+            for (size_t i = 0; i < rest.size(); ++i) sub[i] = order[(size_t)rest[i]];
+            std::vector<BatchPair> bp2;
+            std::vector<int32_t> up2;
+            std::vector<BestRec> pb2;
+            int64_t hb2 = 0;
+            layout_units(info, sub, flags, 32 * R1, bp2, up2, &hb2);
+            rc = run_launch(c, d_seq, tab, base, bp2, up2, hb2, false, R1, pb2, &ms1);
+            if (rc != SWB_OK) return rc;
+            launches += 2;
+            for (size_t i = 0; i < rest.size(); ++i) pbest[(size_t)rest[i]] = pb2[i];
+        }
+    } else if (!order.empty() && !use_graph) {
         BatchArgs a1 = base;
         if (first_stores) {
             layout_stores(bp, out->items, order, &srn, &scn, &ops_total, &xp_total);

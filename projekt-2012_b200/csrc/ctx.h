@@ -45,7 +45,7 @@ struct swb_ctx {
     swb::DevBuf tb[24];  // traceback scratch (ops, crosspoints, state, level-2 stores, recompute and walker buffers)
     // batched path: sequences, encodings, descriptors, per-unit / per-pair records, stores
     swb::DevBuf b_seq, b_rcode, b_ctab, b_pairs, b_units, b_hbuf, b_gbest, b_ubest, b_pbest, b_ctl, b_srows,
-        b_scols, b_walk, b_ops, b_xps, b_state, b_gdir;
+        b_scols, b_walk, b_ops, b_xps, b_state, b_gdir, b_sat;
     swb::HostBuf h_stage;  // pinned staging for descriptors and results
     swb::HostBuf h_io;     // pinned staging of ctx_get / ctx_put
     // graphed batches: the call header (allocated once: the graphs hold its
@@ -79,7 +79,7 @@ struct swb_ctx {
         for (swb::DevBuf *b : {&rows, &cols, &hbuf, &wbest, &best, &errf, &srows, &scols, &work, &flags, &lut,
                                &rcode, &ctab, &trace, &b_seq, &b_rcode, &b_ctab, &b_pairs, &b_units, &b_hbuf,
                                &b_gbest, &b_ubest, &b_pbest, &b_ctl, &b_srows, &b_scols, &b_walk, &b_ops, &b_xps,
-                               &b_state, &b_gdir, &g_hdr, &g_in, &g_work, &g_out, &g_dir})
+                               &b_state, &b_gdir, &b_sat, &g_hdr, &g_in, &g_work, &g_out, &g_dir})
             f(*b);
         for (swb::DevBuf &b : tb) f(b);
     }

@@ -201,3 +201,62 @@ def test_graph_mode_switch_between_alphabets(gpu_ctx):
                 rows, cols, _ = O.orient(a, b)
                 assert O.score_ops(rows, cols, O.scoring(*sc), res.start_row[i], res.start_col[i],
                                    res.ops[i]) == res.score[i]
+
+
+def _packable_batch(seed, n, extra=()):
+    rng = random.Random(seed)
+    pairs = []
+    for _ in range(n):
+        L = rng.choice([40, 300, 600, 1100, 1600, 2400])
+        pairs.append(_mutated(rng, rng.randint(max(1, L // 2), L)))
+    pairs += list(extra)
+    rng.shuffle(pairs)
+    return pairs
+
+
+@pytest.mark.parametrize("tie_flag", [0, swb200.FLAG_TIE_ROWMAJOR])
+def test_packed_16bit_pass_equals_int32_and_oracle(gpu_ctx, monkeypatch, tie_flag):
+    """A batch of >= 2,048 pairs in the table mode runs its scoring pass two pairs
+    per warp in packed 16-bit lanes; every pair gets exactly the int32 pass's
+    result (SWB_BATCH_PACK=0) and, on a sample, the oracle's, under both tie rules;
+    the traced pairs' store pass re-checks the packed scores."""
+    pairs = _packable_batch(21 + tie_flag, 2600, [(b"", b"ACGT"), (b"A" * 600, b"A" * 300)])
+    buf, refs = _pack(pairs)
+    sc = (2, -3, -5, -2)
+    packed = gpu_ctx.batch_align(buf, refs, swb200.scoring(*sc), tie_flag, trace_frac=0.01)
+    monkeypatch.setenv("SWB_BATCH_PACK", "0")
+    plain = gpu_ctx.batch_align(buf, refs, swb200.scoring(*sc), tie_flag, trace_frac=0.01)
+    monkeypatch.delenv("SWB_BATCH_PACK")
+    for f in ("score", "end_row", "end_col", "swapped", "start_row", "start_col", "traced"):
+        assert np.array_equal(getattr(packed, f), getattr(plain, f)), f
+    assert packed.ops == plain.ops
+    tie = O.TIE_ROWMAJOR if tie_flag else O.TIE_REFERENCE
+    rng = random.Random(3)
+    for i in rng.sample(range(len(pairs)), 250):
+        a, b = pairs[i]
+        s, r, c, sw = _oracle(a, b, sc, tie)
+        assert (packed.score[i], packed.end_row[i], packed.end_col[i], bool(packed.swapped[i])) == (s, r, c, sw), i
+
+
+def test_packed_pass_detects_16bit_saturation_and_redoes_in_int32(gpu_ctx, monkeypatch):
+    """With the test flag every pair is packed, also identical pairs of 17,000 bp
+    whose score (2 x 17,000 = 34,000) does not fit 16 bits: the kernel flags
+    them when a column maximum reaches the limit and they are scored again in
+    int32, so the results equal the int32 pass and the exact answer."""
+    rng = random.Random(77)
+    longs = []
+    for L in (17_000, 16_600):
+        s = bytes(rng.choice(b"ACGT") for _ in range(L))
+        longs.append((s, s))
+    pairs = _packable_batch(5, 2100, longs)
+    buf, refs = _pack(pairs)
+    sc = (2, -3, -5, -2)
+    forced = gpu_ctx.batch_align(buf, refs, swb200.scoring(*sc), swb200.FLAG_TEST_PACK_ANY)
+    monkeypatch.setenv("SWB_BATCH_PACK", "0")
+    plain = gpu_ctx.batch_align(buf, refs, swb200.scoring(*sc))
+    monkeypatch.delenv("SWB_BATCH_PACK")
+    assert np.array_equal(forced.score, plain.score)
+    assert np.array_equal(forced.end_row, plain.end_row) and np.array_equal(forced.end_col, plain.end_col)
+    for s, _ in longs:
+        i = next(k for k, p in enumerate(pairs) if p[0] == s and p[1] == s)
+        assert (forced.score[i], forced.end_row[i], forced.end_col[i]) == (2 * len(s), len(s) - 1, len(s) - 1)
