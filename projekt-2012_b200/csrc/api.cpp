@@ -27,8 +27,19 @@ thread_local std::string g_thread_err;
 
 namespace swb {
 
+double trace_now_ms() {
+    static const auto t0 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+bool trace_on() {
+    static const bool on = std::getenv("SWB_SERVE_TRACE") != nullptr;
+    return on;
+}
+
 cudaError_t DevBuf::ensure(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
+    const double t0 = trace_on() ? trace_now_ms() : 0.0;
     if (p) cudaFreeAsync(p, st);
     p = nullptr;
     cap = 0;
@@ -36,6 +47,8 @@ cudaError_t DevBuf::ensure(size_t bytes) {
     cudaError_t e = cudaMallocAsync(&p, want, st);
     if (e == cudaSuccess) cap = want;
     else p = nullptr;
+    if (trace_on() && want >= (64u << 20))
+        std::fprintf(stderr, "swb trace %.1f grow %.1f MB in %.2f ms\n", t0, want / 1e6, trace_now_ms() - t0);
     return e;
 }
 

@@ -87,6 +87,11 @@ struct swb_ctx {
 
 namespace swb {
 
+// Timestamped trace lines on stderr when SWB_SERVE_TRACE is set (milliseconds
+// since the first call): serving iterations, long requests, buffer growth.
+double trace_now_ms();
+bool trace_on();
+
 // Records a one-line error on the context (and the calling thread) and returns code.
 int ctx_fail(swb_ctx *ctx, int code, const char *fmt, ...);
 int ctx_cuda_fail(swb_ctx *ctx, cudaError_t e, const char *what);

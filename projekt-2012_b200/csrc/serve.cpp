@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <deque>
@@ -160,6 +161,7 @@ struct swb_server {
                 off += r->b.size();
             }
             cs->max_blocks = cap_grid ? per_sm * o.reserve_sms : 0;
+            const double tr0 = swb::trace_on() ? swb::trace_now_ms() : 0.0;
             swb_batch_result br{};
             const int rc = swb::batch_align_all_traced(cs, buf.data(), (int64_t)bytes, refs.data(), (int64_t)it.size(),
                                                        &sc, o.flags, &br);
@@ -204,6 +206,9 @@ struct swb_server {
                 }
             }
             swb_batch_result_free(&br);
+            if (swb::trace_on())
+                std::fprintf(stderr, "swb trace %.1f short %zu pairs %.1f ms (cap %d)\n", tr0, it.size(),
+                             swb::trace_now_ms() - tr0, cs->max_blocks);
             {
                 std::lock_guard<std::mutex> lk(mu);
                 for (size_t k = 0; k < it.size(); ++k) {
@@ -241,6 +246,10 @@ struct swb_server {
             const int rc = swb_align_pair(cl, r->a.data(), (int64_t)r->a.size(), r->b.data(), (int64_t)r->b.size(), &sc,
                                           o.flags, &res);
             const std::string msg = rc == SWB_OK ? std::string() : std::string(swb_last_error(cl));
+            if (swb::trace_on())
+                std::fprintf(stderr, "swb trace %.1f long %lld x %lld stage1 %.1f stage2 %.1f total %.1f ms\n",
+                             swb::trace_now_ms() - res.total_ms, (long long)r->m, (long long)r->n, res.stage1_ms,
+                             res.stage2_ms, res.total_ms);
             {
                 std::lock_guard<std::mutex> lk(mu);
                 long_active = false;

@@ -28,7 +28,8 @@ SWB_ENOTFOUND = 8
 FLAG_TIE_ROWMAJOR = 0x1
 FLAG_SCORE_ONLY = 0x2
 FLAG_NO_SPECIAL = 0x4
-FLAG_TEST_WITHHOLD = 0x80000000  # test hook (include/swb200.h)
+FLAG_TEST_WITHHOLD = 0x80000000  # test hooks (include/swb200.h)
+FLAG_TEST_PACK_ANY = 0x40000000
 
 
 class Scoring(C.Structure):
@@ -223,7 +224,7 @@ class Batch:
     swapped: "object"
     traced: "object"
     ops: List[str]             # "" for pairs that were not traced
-    xpoints: List[list]        # () for pairs that were not traced
+    xpoints: "object"           # xpoints[i]: list of (row, col, score, gap); () if not traced
     xpoint_interval: "object"
     n_traced: int
     cells: int
@@ -250,14 +251,11 @@ def _convert_batch(r: BatchResult) -> Batch:
     ops_off, n_ops = col("ops_off", np.int64), col("n_ops", np.int64)
     xp_off, n_xp = col("xp_off", np.int64), col("n_xpoints", np.int64)
     allops = C.string_at(r.ops, r.ops_bytes).decode() if r.ops and r.ops_bytes > 0 else ""
-    allxp = _xpoint_tuples(r.xpoints, 0, r.n_xpoints)
     ops = [""] * n
-    xps = [()] * n  # one shared empty tuple for the pairs that were not traced
     idx = np.flatnonzero(traced)
-    for i, o, no, x, nx in zip(idx.tolist(), ops_off[idx].tolist(), n_ops[idx].tolist(), xp_off[idx].tolist(),
-                               n_xp[idx].tolist()):
+    for i, o, no in zip(idx.tolist(), ops_off[idx].tolist(), n_ops[idx].tolist()):
         ops[i] = allops[o:o + no]
-        xps[i] = allxp[x:x + nx]
+    xps = _PairXpoints(_xpoint_array(r.xpoints, r.n_xpoints), xp_off, np.where(traced != 0, n_xp, 0))
     return Batch(score, col("end_row", np.int64), col("end_col", np.int64), col("start_row", np.int64),
                  col("start_col", np.int64), swapped.astype(bool), traced.astype(bool), ops, xps, xpi,
                  r.n_traced, r.cells, r.stage1_ms, r.stage2_ms, r.total_ms, r.kernel_launches)
@@ -273,6 +271,19 @@ def pair_refs(refs) -> "C.Array":
     return arr
 
 
+def _xpoint_array(ptr, count: int):
+    """The count XPoint records at ptr as a numpy structured array in (row, col,
+    score, gap) field order (a copy; tolist() of a slice gives the tuples)."""
+    import numpy as np
+    size = C.sizeof(XPoint)
+    dt = np.dtype({"names": ["row", "col", "score", "gap"], "formats": [np.int64, np.int64, np.int32, np.int32],
+                   "offsets": [XPoint.row.offset, XPoint.col.offset, XPoint.score.offset, XPoint.gap.offset],
+                   "itemsize": size})
+    if count <= 0 or not ptr:
+        return np.zeros(0, dtype=dt)
+    return np.frombuffer(C.string_at(C.cast(ptr, C.c_void_p).value, count * size), dtype=dt)
+
+
 def _xpoint_tuples(ptr, first: int, count: int) -> list:
     """(row, col, score, gap) tuples of count XPoint records starting at ptr[first]."""
     if count <= 0 or not ptr:
@@ -285,6 +296,29 @@ def _xpoint_tuples(ptr, first: int, count: int) -> list:
                    "offsets": [XPoint.row.offset, XPoint.col.offset, XPoint.score.offset, XPoint.gap.offset],
                    "itemsize": size})
     return np.frombuffer(raw, dtype=dt).tolist()
+
+
+class _PairXpoints:
+    """Per-pair crosspoint lists of a batch, built on access: xp[i] is the list of
+    (row, col, score, gap) tuples of pair i (() for pairs that were not traced).
+    A batch with 1,000 traced pairs holds about 500,000 crosspoints; turning all
+    of them into tuples up front took 100 ms per call."""
+
+    def __init__(self, raw, off, cnt):
+        self._raw, self._off, self._cnt = raw, off, cnt
+
+    def __len__(self):
+        return len(self._off)
+
+    def __getitem__(self, i):
+        n = int(self._cnt[i])
+        if n <= 0:
+            return ()
+        o = int(self._off[i])
+        return self._raw[o:o + n].tolist()
+
+    def __iter__(self):
+        return (self[i] for i in range(len(self)))
 
 
 def _convert(r: Result) -> Alignment:
