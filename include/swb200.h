@@ -101,6 +101,7 @@ typedef struct {
     int32_t     special_interval;   /* rows between this run's HBM special rows     */
     int64_t     special_bytes;      /* HBM held by special rows for this call       */
     int32_t     kernel_launches;    /* this library's kernels launched by the call  */
+    int64_t     host_bytes;         /* of special_bytes, kept in pinned host memory */
 } swb_result;
 
 typedef struct {
@@ -116,6 +117,13 @@ typedef struct {
                                        and the call returns SWB_ETIMEOUT (the
                                        reference exits -2 on any CUDA error,
                                        src/SWutils.cpp:19-24); 0 = 20,000 ms      */
+    uint64_t host_spill_bytes;      /* pinned host memory the special rows or columns
+                                       of one call may use beyond hbm_budget_bytes
+                                       (the reference appends its special rows to
+                                       disk files, src/Builders.cpp:41-61); the
+                                       kernels write them through a mapped pointer
+                                       and the traceback reads its blocks back;
+                                       0 = none (over the budget: level-1 grid)  */
 } swb_options;
 
 typedef struct swb_ctx swb_ctx;

@@ -75,6 +75,28 @@ void HostBuf::release() {
     cap = 0;
 }
 
+cudaError_t MappedBuf::ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    release();
+    cudaError_t e = cudaHostAlloc(&p, bytes < 256 ? 256 : bytes, cudaHostAllocMapped | cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return e;
+    }
+    if ((e = cudaHostGetDevicePointer(&dp, p, 0)) != cudaSuccess) {
+        release();
+        return e;
+    }
+    cap = bytes < 256 ? 256 : bytes;
+    return cudaSuccess;
+}
+
+void MappedBuf::release() {
+    if (p) cudaFreeHost(p);
+    p = dp = nullptr;
+    cap = 0;
+}
+
 int ctx_fail(swb_ctx *ctx, int code, const char *fmt, ...) {
     char buf[512];
     va_list ap;
@@ -212,6 +234,8 @@ void swb_ctx_destroy(swb_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->h_stage.release();
     c->h_io.release();
+    c->srows_h.release();
+    c->scols_h.release();
     c->h_gin.release();
     c->h_gout.release();
     for (auto &g : c->graphs) {
@@ -419,19 +443,36 @@ int run_stage1(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_co
             a.nsc = nsc;
         }
     }
-    if (sbytes > c->opts.hbm_budget_bytes)
-        return ctx_fail(c, SWB_ENOMEM_BUDGET, "special rows and columns need %zu bytes > budget %llu", sbytes,
-                    (unsigned long long)c->opts.hbm_budget_bytes);
+    const size_t rows_bytes = sizeof(int2) * (size_t)a.nsr * (size_t)n;
+    const size_t cols_bytes = sizeof(int2) * (size_t)a.nsc * (size_t)m;
+    bool rows_host = false, cols_host = false;
+    if (!tb::spill_placement(c->opts.hbm_budget_bytes, c->opts.host_spill_bytes, rows_bytes, cols_bytes, &rows_host,
+                             &cols_host))
+        return ctx_fail(c, SWB_ENOMEM_BUDGET, "special rows and columns need %zu bytes > budget %llu + spill %llu",
+                        sbytes, (unsigned long long)c->opts.hbm_budget_bytes,
+                        (unsigned long long)c->opts.host_spill_bytes);
+    c->last_host_bytes = (int64_t)((rows_host ? rows_bytes : 0) + (cols_host ? cols_bytes : 0));
     if (a.nsr > 0) {
-        if ((e = c->srows.ensure(sizeof(int2) * (size_t)a.nsr * (size_t)n)) != cudaSuccess)
-            return ctx_cuda_fail(c, e, "special rows");
-        a.srows = (int2 *)c->srows.p;
+        if (rows_host) {
+            if ((e = c->srows_h.ensure(rows_bytes)) != cudaSuccess) return ctx_cuda_fail(c, e, "spilled special rows");
+            a.srows = (int2 *)c->srows_h.dp;
+        } else {
+            if ((e = c->srows.ensure(rows_bytes)) != cudaSuccess) return ctx_cuda_fail(c, e, "special rows");
+            a.srows = (int2 *)c->srows.p;
+        }
     }
     if (a.nsc > 0) {
-        if ((e = c->scols.ensure(sizeof(int2) * (size_t)a.nsc * (size_t)m)) != cudaSuccess)
-            return ctx_cuda_fail(c, e, "special columns");
-        a.scols = (int2 *)c->scols.p;
+        if (cols_host) {
+            if ((e = c->scols_h.ensure(cols_bytes)) != cudaSuccess)
+                return ctx_cuda_fail(c, e, "spilled special columns");
+            a.scols = (int2 *)c->scols_h.dp;
+        } else {
+            if ((e = c->scols.ensure(cols_bytes)) != cudaSuccess) return ctx_cuda_fail(c, e, "special columns");
+            a.scols = (int2 *)c->scols.p;
+        }
     }
+    c->last_srows = a.srows;
+    c->last_scols = a.scols;
     c->last_nsr = a.nsr;
     c->last_n = n;
     c->last_sr_interval = a.nsr > 0 ? a.sr_every * plan.strip_rows : 0;
@@ -494,6 +535,7 @@ int align_device(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_
     out->special_interval = (int32_t)c->last_sr_interval;
     if (!score_only && sr_interval < 0) plan = tb::plan_for(c->opts, m, n, c->last_sr_interval);
     out->special_bytes = (int64_t)sizeof(int2) * nsr * n + (sc_interval > 0 ? (int64_t)sizeof(int2) * (n / sc_interval) * m : 0);
+    out->host_bytes = c->last_host_bytes;
     if (best.valid) {
         out->score = best.ho - sc->gap_open;
         out->end_row = best.row;
@@ -523,8 +565,8 @@ int align_device(swb_ctx *c, const uint8_t *d_rows, int64_t m, const uint8_t *d_
         // a capped context (the serving loop's long lane) sizes its stage-2 grids
         // to the same share of the GPU as its stage 1 (4 scoring blocks per SM)
         const int tb_sms = c->max_blocks > 0 ? std::max(1, std::min(c->sms, c->max_blocks / 4)) : c->sms;
-        rc = tb::traceback(c->stream, tb_sms, d_rows, m, d_cols, n, sc, plan, (const int2 *)c->srows.p,
-                           (const int2 *)c->scols.p, out, scr, c->err, &launches);
+        rc = tb::traceback(c->stream, tb_sms, d_rows, m, d_cols, n, sc, plan, c->last_srows, c->last_scols, out, scr,
+                           c->err, &launches);
         if (rc != SWB_OK) return ctx_fail(c, rc, "%s", c->err.c_str());
         out->kernel_launches += launches;
         out->stage2_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
@@ -624,7 +666,7 @@ extern "C" int swb_special_row_copy(swb_ctx *c, int64_t idx, int32_t *out, int64
     if (idx < 0 || idx >= c->last_nsr || cols != c->last_n)
         return ctx_fail(c, SWB_EINVAL, "special row %lld not available", (long long)idx);
     cudaSetDevice(c->device);
-    cudaError_t e = swb::ctx_get(c, out, (const int2 *)c->srows.p + idx * c->last_n, sizeof(int2) * (size_t)cols);
+    cudaError_t e = swb::ctx_get(c, out, c->last_srows + idx * c->last_n, sizeof(int2) * (size_t)cols);
     if (e != cudaSuccess) return ctx_cuda_fail(c, e, "special row copy");
     return SWB_OK;
 }

@@ -23,6 +23,15 @@ struct DevBuf {
     void release();
 };
 
+// Pinned host memory mapped into the device's address space (special rows or
+// columns spilled beyond the HBM budget); dp is the address kernels use.
+struct MappedBuf {
+    void *p = nullptr, *dp = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes);
+    void release();
+};
+
 // A pinned host allocation that grows on demand.
 struct HostBuf {
     void *p = nullptr;
@@ -46,6 +55,9 @@ struct swb_ctx {
     // batched path: sequences, encodings, descriptors, per-unit / per-pair records, stores
     swb::DevBuf b_seq, b_rcode, b_ctab, b_pairs, b_units, b_hbuf, b_gbest, b_ubest, b_pbest, b_ctl, b_srows,
         b_scols, b_walk, b_ops, b_xps, b_state, b_gdir, b_sat;
+    swb::MappedBuf srows_h, scols_h;  // special rows / columns spilled to pinned host memory
+    int2 *last_srows = nullptr, *last_scols = nullptr;  // where the last stage 1 kept them
+    int64_t last_host_bytes = 0;
     swb::HostBuf h_stage;  // pinned staging for descriptors and results
     swb::HostBuf h_io;     // pinned staging of ctx_get / ctx_put
     // graphed batches: the call header (allocated once: the graphs hold its

@@ -657,12 +657,24 @@ cudaError_t walker_configure() {
     return e;
 }
 
+bool spill_placement(uint64_t hbm, uint64_t spill, uint64_t rows_bytes, uint64_t cols_bytes, bool *rows_host,
+                     bool *cols_host) {
+    *rows_host = *cols_host = false;
+    if (rows_bytes + cols_bytes <= hbm) return true;
+    if (rows_bytes <= spill && cols_bytes <= hbm) return *rows_host = true;
+    if (cols_bytes <= spill && rows_bytes <= hbm) return *cols_host = true;
+    if (rows_bytes + cols_bytes <= spill) return *rows_host = *cols_host = true;
+    return false;
+}
+
 Plan plan_for(const swb_options &opts, int64_t m, int64_t n, int64_t br) {
     Plan p;
     if (br <= 0 || br > kBR || br % 32 != 0) br = kBR;
     const double budget = (double)(opts.hbm_budget_bytes ? opts.hbm_budget_bytes : (64ULL << 30));
-    const double direct = 8.0 * ((double)(m / br) * (double)n + (double)(n / kBC) * (double)m);
-    if (direct <= budget) {
+    const uint64_t rows_bytes = 8ULL * (uint64_t)(m / br) * (uint64_t)n;
+    const uint64_t cols_bytes = 8ULL * (uint64_t)(n / kBC) * (uint64_t)m;
+    bool rh = false, ch = false;
+    if (spill_placement((uint64_t)budget, opts.host_spill_bytes, rows_bytes, cols_bytes, &rh, &ch)) {
         p.level1 = false;
         p.kr = br;
         p.kc = kBC;

@@ -23,6 +23,12 @@ struct Plan {
 // br: the stage-1 strip height the special rows will come from (a multiple of 32
 // up to 512); direct mode when its stores fit the budget.
 Plan plan_for(const swb_options &opts, int64_t m, int64_t n, int64_t br = 512);
+// Where direct-mode special rows and columns go: both in HBM when they fit the
+// budget; else one set (rows first) in pinned host memory when it fits the
+// spill and the other fits the budget; else both in host memory when they fit
+// the spill.  Returns false when none of these fits (level-1 grid instead).
+bool spill_placement(uint64_t hbm, uint64_t spill, uint64_t rows_bytes, uint64_t cols_bytes, bool *rows_host,
+                     bool *cols_host);
 // Level-1 traceback: cells recomputed per corridor round, and device bytes per
 // cell (its 512 x 256 stores and row hand-off buffer).
 int64_t level1_corridor_cells(const Plan &plan, int sms);

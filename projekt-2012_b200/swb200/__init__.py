@@ -51,7 +51,7 @@ class Result(C.Structure):
                 ("n_ops", C.c_int64), ("ops", C.c_void_p),
                 ("n_xpoints", C.c_int64), ("xpoints", C.POINTER(XPoint)),
                 ("xpoint_interval", C.c_int32), ("special_interval", C.c_int32),
-                ("special_bytes", C.c_int64), ("kernel_launches", C.c_int32)]
+                ("special_bytes", C.c_int64), ("kernel_launches", C.c_int32), ("host_bytes", C.c_int64)]
 
 
 class PairRef(C.Structure):
@@ -100,7 +100,7 @@ class ServerStats(C.Structure):
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64),
                 ("special_interval", C.c_int32), ("verbose", C.c_int32),
-                ("cuda_stream", C.c_uint64), ("wait_limit_ms", C.c_uint32)]
+                ("cuda_stream", C.c_uint64), ("wait_limit_ms", C.c_uint32), ("host_spill_bytes", C.c_uint64)]
 
 
 class SwbError(RuntimeError):
@@ -210,6 +210,7 @@ class Alignment:
     special_bytes: int = 0
     kernel_launches: int = 0
     n_ops: int = 0
+    host_bytes: int = 0      # of special_bytes, kept in pinned host memory
 
 
 @dataclass
@@ -327,7 +328,7 @@ def _convert(r: Result) -> Alignment:
     return Alignment(r.score, r.end_row, r.end_col, r.start_row, r.start_col, bool(r.swapped),
                      r.rows, r.cols, r.stage1_ms, r.stage2_ms, r.total_ms, ops, xps,
                      r.xpoint_interval, r.special_interval, r.special_bytes, r.kernel_launches,
-                     r.n_ops)
+                     r.n_ops, r.host_bytes)
 
 
 FASTA_MULTI = 0x1
@@ -403,7 +404,7 @@ class Context:
     """One device context (owns a CUDA stream and reusable device buffers)."""
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, special_interval: int = 0,
-                 cuda_stream: int = 0, verbose: int = 0, wait_limit_ms: int = 0):
+                 cuda_stream: int = 0, verbose: int = 0, wait_limit_ms: int = 0, host_spill_bytes: int = 0):
         L = lib()
         o = Options()
         L.swb_options_default(C.byref(o))
@@ -413,6 +414,7 @@ class Context:
         o.cuda_stream = cuda_stream
         o.verbose = verbose
         o.wait_limit_ms = wait_limit_ms
+        o.host_spill_bytes = host_spill_bytes
         h = C.c_void_p()
         rc = L.swb_ctx_create(C.byref(o), C.byref(h))
         if rc != SWB_OK:

@@ -1,7 +1,8 @@
 """The full-size pairs on the GPU.  The 1 Mbp pair's score and end cell are
 pinned by the oracle's full CPU wavefront (tests/golden/long_pair_golden.json,
 made by tests/golden/make_long_pair_golden.py, both tie rules); its alignment and
-the 10 Mbp pair's are checked through properties that hold at any size: the
+the 10 Mbp pair's (whose score and end cell the oracle's AVX-512 wavefront pins,
+tests/golden/chromosome_golden.json) are checked through properties that hold at any size: the
 operations re-score to the reported score from a start cell to the end cell, the
 crosspoints lie on the path with its prefix score on every special row, and
 stage 1 gives the same result with another tile height."""
@@ -81,6 +82,13 @@ def test_chromosome_pair_10mbp_properties():
         res = ctx.align(a, b, swb200.scoring(*sc))
         rows, cols = (b, a) if res.swapped else (a, b)
         _path_check(rows, cols, sc, res)
+        # the oracle's full-matrix result (AVX-512 wavefront over all 10^14 cells)
+        gpath = os.path.join(GOLDEN, "chromosome_golden.json")
+        if os.path.exists(gpath):
+            g = json.load(open(gpath))
+            assert g["sha256_a"] == hashlib.sha256(a).hexdigest() and g["sha256_b"] == hashlib.sha256(b).hexdigest()
+            assert (res.score, res.end_row, res.end_col) == \
+                (g["reference"]["score"], g["reference"]["end_row"], g["reference"]["end_col"])
         # stage 1 alone, with the other tile height, gives the same score and end cell
         os.environ["SWB_STAGE1_R"] = "8"
         try:

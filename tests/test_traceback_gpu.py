@@ -196,3 +196,32 @@ def test_cli_block_equals_the_reference_renderer(tmp_path, fixture):
     rows, cols, _ = O.orient(load_fixture_fasta(fa), load_fixture_fasta(fb))
     ref = O.run_reference_visual(rows, cols, prefix + ".first.bin", prefix + ".second.bin", start, end)
     assert block == ref
+
+
+def test_special_rows_and_columns_spilled_to_pinned_host_memory():
+    """Stores over the HBM budget but within budget + host_spill_bytes stay on the
+    direct grid with the special rows, the special columns or both in mapped
+    pinned host memory (the reference appends its special rows to disk files,
+    src/Builders.cpp:41-61): the same alignment, start and crosspoints as with
+    everything in HBM, and the oracle's score and end cell."""
+    rng = random.Random(12)
+    a, b = _similar_pair(rng, 60_000, 0.7, sub=0.05, indel=0.01)
+    sc = swb200.scoring(1, -3, -5, -2)
+    with swb200.Context(device=0) as ctx:
+        full = ctx.align(a, b, sc)
+    assert full.host_bytes == 0 and full.special_interval in (448, 512)
+    rows_b = 8 * (max(len(a), len(b)) // full.special_interval) * min(len(a), len(b))
+    cols_b = 8 * (min(len(a), len(b)) // 256) * max(len(a), len(b))
+    for budget, spill, expect in [(cols_b + 1024, rows_b + (1 << 20), rows_b),   # rows to the host
+                                  (rows_b + 1024, cols_b + (1 << 20), cols_b),   # columns to the host
+                                  (1 << 20, rows_b + cols_b + (1 << 21), rows_b + cols_b)]:
+        with swb200.Context(device=0, hbm_budget_bytes=budget, host_spill_bytes=spill) as ctx:
+            r = ctx.align(a, b, sc)
+        assert r.special_interval == full.special_interval  # the direct grid, not level 1
+        assert r.host_bytes == expect, (budget, spill, r.host_bytes)
+        assert (r.score, r.end_row, r.end_col, r.start_row, r.start_col) == \
+            (full.score, full.end_row, full.end_col, full.start_row, full.start_col)
+        assert r.ops == full.ops and r.xpoints == full.xpoints
+    rows, cols, _ = O.orient(a, b)
+    e = O.stage1_fast(rows, cols, O.scoring(1, -3, -5, -2), O.TIE_REFERENCE)[0]
+    assert (full.score, full.end_row, full.end_col) == (e.score, e.row, e.col)
