@@ -299,6 +299,26 @@ int swb_server_create(const swb_server_options *opts, const swb_scoring *sc, swb
         delete s;
         return rc;
     }
+    // Device memory mapped up front.  Buffers grow stream-ordered (cudaMallocAsync),
+    // but a growth the device's pool cannot serve from memory it already holds
+    // maps new memory, which took 0.2 - 1.1 s for the long lane's 19 - 33 GB
+    // special-row buffers and held up the short lane's launches meanwhile (the
+    // serving loop's short-request tail).  So the pool keeps what is freed
+    // (release threshold: never) and is grown once, here, to the admission budget.
+    {
+        cudaMemPool_t pool;
+        uint64_t keep = ~0ULL;
+        void *warm = nullptr;
+        cudaSetDevice(s->o.device);
+        if (cudaDeviceGetDefaultMemPool(&pool, s->o.device) == cudaSuccess &&
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess &&
+            cudaMallocAsync(&warm, (size_t)s->o.hbm_budget_bytes, s->cl->stream) == cudaSuccess) {
+            cudaFreeAsync(warm, s->cl->stream);
+            cudaStreamSynchronize(s->cl->stream);
+        } else {
+            cudaGetLastError();  // not fatal: buffers then grow on demand as before
+        }
+    }
     // pinned staging sized up front: growing it later (cudaFreeHost) would stall the device
     if (s->cs->h_io.ensure(64ULL << 20) != cudaSuccess || s->cl->h_io.ensure(64ULL << 20) != cudaSuccess ||
         s->cs->h_stage.ensure(16ULL << 20) != cudaSuccess) {

@@ -321,6 +321,9 @@ class _PairXpoints:
     def __iter__(self):
         return (self[i] for i in range(len(self)))
 
+    def __eq__(self, other):
+        return len(self) == len(other) and all(x == y for x, y in zip(self, other))
+
 
 def _convert(r: Result) -> Alignment:
     ops = C.string_at(r.ops, r.n_ops).decode() if r.n_ops > 0 and r.ops else ""
