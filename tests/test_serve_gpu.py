@@ -91,3 +91,31 @@ def test_wait_timeout_and_destroy_with_queued_requests():
     r = srv.wait(ids[0], 0)          # may or may not be done: either a result or None
     assert r is None or r[0].score >= 0
     srv.close()                      # queued requests are dropped, running ones finish
+
+
+def test_serving_mix_stream_results_equal_the_plain_path(gpu_ctx):
+    """A seeded stretch of the serving workload's own stream (synth.serving_stream:
+    Poisson arrivals, 95% short pairs of 200-5,000 bp, 5% long pairs of 100 kbp -
+    2 Mbp, scoring 1/-3/-5/-2, full traceback, 100 GB budget) submitted at its
+    arrival times: every result, long or short, equals the plain path's on the
+    same pair alone."""
+    from swb200 import synth
+    stream = synth.serving_stream(6.0, 12.0, seed_extra=7)
+    assert any(lg for *_, lg in stream) and sum(1 for *_, lg in stream if not lg) > 40
+    sc = swb200.scoring(*SC)
+    ids = []
+    with swb200.Server(sc, hbm_budget_bytes=100 << 30) as srv:
+        start = time.perf_counter()
+        for t_arr, q, tg, _ in stream:
+            now = time.perf_counter() - start
+            if t_arr > now:
+                time.sleep(t_arr - now)
+            ids.append(srv.submit(q, tg))
+        got = [srv.wait(i) for i in ids]
+        st = srv.stats()
+    assert st["completed"] == len(stream) and st["failed"] == 0
+    with swb200.Context(device=0, hbm_budget_bytes=50 << 30) as ctx:
+        for (t_arr, q, tg, lg), (res, info) in zip(stream, got):
+            assert info["lane"] == (1 if lg else 0)
+            alone = ctx.align(q, tg, sc)
+            assert _same(res, alone), (len(q), len(tg), lg)
