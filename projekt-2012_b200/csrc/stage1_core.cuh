@@ -105,27 +105,25 @@ __device__ __forceinline__ int32_t slow_best(uint32_t mask, int32_t cm, const Ti
                                           int64_t c_origin, Best *b, int64_t row0, int32_t j, int32_t *gbest,
                                           int32_t open) {
     const int32_t before = b->ho;
-    if (row0 + 32 > m) mask &= (m - row0 > 0) ? (uint32_t)((1ULL << (m - row0)) - 1ULL) : 0u;  // rows past the end
-    if (mask == 0) return b->ho;
-    if (cm > b->ho && (mask & (mask - 1)) == 0) {
-        // strictly better than anything this lane holds, and a single cell
-        b->ho = cm;
-        b->keyed = 0;
-        b->row = row0 + __ffs(mask) - 1;
-        b->col = j;
-    } else {
+    while (mask) {
+        const int i = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const int64_t r = row0 + i;
+        if (r >= m) break;
+        if (cm > b->ho) {  // strictly better: its key is needed only if a tie comes later
+            b->ho = cm;
+            b->keyed = 0;
+            b->row = r;
+            b->col = j;
+            continue;
+        }
+        // cm == b->ho (the candidate test admits nothing below the lane's best)
         key_best(b, tie, r_origin, c_origin);
-        while (mask) {
-            const int i = __ffs(mask) - 1;
-            mask &= mask - 1;
-            const int64_t r = row0 + i;
-            const uint64_t key = tie_key(tie, r_origin + r, c_origin + j);
-            if (better(cm, key, b->ho, b->key)) {
-                b->ho = cm;
-                b->key = key;
-                b->row = r;
-                b->col = j;
-            }
+        const uint64_t key = tie_key(tie, r_origin + r, c_origin + j);
+        if (key < b->key) {
+            b->key = key;
+            b->row = r;
+            b->col = j;
         }
     }
     if (b->ho > before) atomicMax(gbest, b->ho - open);
@@ -362,7 +360,8 @@ __device__ bool run_strip(const A &a, int4 *ring, int4 *stage, int lane, int32_t
     sc.strip = s;
     sc.n = (int32_t)a.n;
     sc.below = (int64_t)(s + 1) * H < a.m && !(a.withhold && s == 0);
-    sc.last_row = a.bottom != nullptr && (int64_t)(s + 1) * H == a.m;
+    // the block outputs (swb_score_block_device) come from score-only launches
+    sc.last_row = !STORES && a.bottom != nullptr && (int64_t)(s + 1) * H == a.m;
     sc.sr = a.srows != nullptr && ((int64_t)(s + 1) % a.sr_every) == 0 && (int64_t)(s + 1) * H <= a.m;
     sc.sr_off = sc.sr ? ((int64_t)(s + 1) / a.sr_every - 1) * a.n : 0;
     L.bho = bho;
@@ -462,7 +461,7 @@ __device__ bool run_strip(const A &a, int4 *ring, int4 *stage, int lane, int32_t
     // the columns staged since the last refill
     flush(a, stage, lane, sc, n, ((kEnd + kCH - 1) / kCH) * kCH);
     __syncwarp();
-    if (a.right != nullptr) {
+    if (!STORES && a.right != nullptr) {
         // after its last column a lane's registers hold H + open and E of column n - 1
 #pragma unroll
         for (int i = 0; i < R; ++i)
