@@ -12,6 +12,14 @@
 // every new entry appended, so later processes skip the probes.  The special-row
 // spacing is the other tuned parameter; it is chosen from the HBM budget by the
 // traceback planner (the densest grid that fits).
+//
+// Batches: the packed 16-bit pass takes 448- or 256-row strips.  Short pairs pad
+// less with 256 rows, long ones run fewer per-strip steps with 448, so the
+// choice depends on the batch's length mix.  Its bucket is the SM count and
+// ceil(log2) of the cells-weighted median rows and columns of the packed pairs;
+// batch_host.cpp times each candidate on a strided sample of the batch's own
+// pairs (the samples' results are kept) and records the faster here, in the
+// same table and file.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -71,6 +79,27 @@ void store_locked(const std::string &key, int R) {
 }
 
 }  // namespace
+
+std::string batch_tune_key(int sms, const char *pass, int64_t m, int64_t n) {
+    char k[96];
+    snprintf(k, sizeof k, "sms%d %s tab r%d c%d", sms, pass, log2ceil(m), log2ceil(n));
+    return k;
+}
+
+bool tune_lookup(const std::string &key, int *R) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    load_locked();
+    auto it = g_table.find(key);
+    if (it == g_table.end()) return false;
+    *R = it->second;
+    return true;
+}
+
+void tune_record(const std::string &key, int R) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    load_locked();
+    store_locked(key, R);
+}
 
 int autotune_rows_per_lane(swb_ctx *c, const Stage1Args &base, bool tab, bool stores, int fallback,
                            bool strip_rows, int64_t sr_interval) {

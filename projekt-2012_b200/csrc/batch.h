@@ -87,10 +87,14 @@ struct Batch16Args {
     int64_t wait_limit;
 };
 
-constexpr int kBatch16R = 14;  // rows per lane of the packed kernel
+// Rows per lane of the packed kernel: 14 (448-row strips) unless the batch
+// autotuner picks 8 (256-row strips, less padding below short pairs).
+constexpr int kBatch16R = 14;
+constexpr int kBatch16RShort = 8;
 
 cudaError_t batch16_configure();
-cudaError_t batch16_launch(const Batch16Args &a, int sms, int max_blocks, int64_t npacked, BestRec *pbest,
+// R: kBatch16R or kBatch16RShort; the packed pairs' strip counts must use it.
+cudaError_t batch16_launch(const Batch16Args &a, int R, int sms, int max_blocks, int64_t npacked, BestRec *pbest,
                            cudaStream_t st);
 
 // Rows per lane of the batched kernel's store passes (their strips are 512 rows,

@@ -108,7 +108,7 @@ __device__ __forceinline__ void flush16(const Batch16Args &g, const PackedPair &
 }
 
 // Half h of the column maximum reached the threshold at column j: record the
-// rows holding it (lazy tie keys, as slow_best), flag saturation.
+// rows holding it (lazy tie keys, as slow_best_single), flag saturation.
 template <int R>
 __device__ __forceinline__ void slow16(Lane16<R> &L, const Batch16Args &g, const PackedPair &d, Best *b, int h,
                                        uint32_t cm, int64_t row0, int32_t j) {
@@ -118,7 +118,7 @@ __device__ __forceinline__ void slow16(Lane16<R> &L, const Batch16Args &g, const
     uint32_t mask = 0;
 #pragma unroll
     for (int i = 0; i < R; ++i) mask |= (half(L.HO[i], h) == c ? 1u : 0u) << i;
-    const int32_t bho = slow_best(mask, c, d.tie[h], d.m[h], 0, 0, b, row0, j, g.gbest + d.slot[h], g.open);
+    const int32_t bho = slow_best_single(mask, c, d.tie[h], d.m[h], 0, 0, b, row0, j, g.gbest + d.slot[h], g.open);
     const int32_t t = half(L.thr, h);
     const int32_t nt = max(t, bho);
     L.thr = h == 0 ? ((L.thr & 0xFFFF0000u) | (uint32_t)(uint16_t)(int16_t)nt)
@@ -376,19 +376,22 @@ cudaError_t batch16_configure() {
     const int c = cudaSharedmemCarveoutMaxShared;
     const auto A = cudaFuncAttributePreferredSharedMemoryCarveout;
     cudaError_t e = cudaFuncSetAttribute((const void *)batch16_kernel<kBatch16R>, A, c);
+    cudaError_t e1 = cudaFuncSetAttribute((const void *)batch16_kernel<kBatch16RShort>, A, c);
     cudaError_t e2 = cudaFuncSetAttribute((const void *)batch16_reduce_kernel, A, c);
-    return e != cudaSuccess ? e : e2;
+    return e != cudaSuccess ? e : (e1 != cudaSuccess ? e1 : e2);
 }
 
-cudaError_t batch16_launch(const Batch16Args &a, int sms, int max_blocks, int64_t npacked, BestRec *pbest,
+cudaError_t batch16_launch(const Batch16Args &a, int R, int sms, int max_blocks, int64_t npacked, BestRec *pbest,
                            cudaStream_t st) {
+    if (R != kBatch16R && R != kBatch16RShort) return cudaErrorInvalidValue;
     if (a.nunits > 0) {
-        const int per_sm = std::max(1, max_blocks16<kBatch16R>());
+        const int per_sm = std::max(1, R == kBatch16R ? max_blocks16<kBatch16R>() : max_blocks16<kBatch16RShort>());
         const int64_t need = (a.nunits + kWarps - 1) / kWarps;
         int64_t limit = (int64_t)per_sm * sms;
         if (max_blocks > 0 && max_blocks < limit) limit = max_blocks;
         const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(need, limit));
-        batch16_kernel<kBatch16R><<<blocks, kWarps * 32, 0, st>>>(a);
+        if (R == kBatch16R) batch16_kernel<kBatch16R><<<blocks, kWarps * 32, 0, st>>>(a);
+        else batch16_kernel<kBatch16RShort><<<blocks, kWarps * 32, 0, st>>>(a);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }

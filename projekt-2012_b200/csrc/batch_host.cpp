@@ -190,15 +190,16 @@ bool packing_enabled() {
 // it is packed without that risk.
 constexpr int32_t kSatLimit = 32767 - 256;
 
-// The packed scoring pass over the positions `pos` of `order`: pairs sorted by
-// strip count and width and taken two at a time (a pair whose neighbour has
-// another strip count gets an empty partner).  Fills pbest[k] for every k in
-// pos and appends to `redo` the positions whose pair reached the 16-bit limit.
+// The packed scoring pass over the positions `pos` of `order` with R rows per
+// lane: pairs sorted by strip count and width and taken two at a time (a pair
+// whose neighbour has another strip count gets an empty partner).  Fills
+// pbest[k] for every k in pos and appends to `redo` the positions whose pair
+// reached the 16-bit limit.
 int run_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &info,
-               const std::vector<int64_t> &order, std::vector<int64_t> pos, uint32_t flags,
+               const std::vector<int64_t> &order, std::vector<int64_t> pos, uint32_t flags, int R,
                std::vector<BestRec> &pbest, std::vector<int64_t> &redo, float *ms) {
     cudaError_t e;
-    const int64_t H = 32LL * kBatch16R;
+    const int64_t H = 32LL * R;
     auto strips = [&](int64_t k) { return (info[(size_t)order[(size_t)k]].m + H - 1) / H; };
     std::stable_sort(pos.begin(), pos.end(), [&](int64_t x, int64_t y) {
         const int64_t sx = strips(x), sy = strips(y);
@@ -290,7 +291,7 @@ int run_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &i
         (e = cudaMemsetAsync(a.ctl, 0, 4 * sizeof(int32_t), c->stream)) != cudaSuccess)
         return ctx_cuda_fail(c, e, "packed batch set-up");
     cudaEventRecord(c->ev0, c->stream);
-    if ((e = batch16_launch(a, c->sms, c->max_blocks, np, (BestRec *)c->b_pbest.p, c->stream)) != cudaSuccess)
+    if ((e = batch16_launch(a, R, c->sms, c->max_blocks, np, (BestRec *)c->b_pbest.p, c->stream)) != cudaSuccess)
         return ctx_cuda_fail(c, e, "packed batch launch");
     cudaEventRecord(c->ev1, c->stream);
     BestRec *hb_best = (BestRec *)hs;
@@ -311,6 +312,83 @@ int run_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &i
     float t = 0.f;
     cudaEventElapsedTime(&t, c->ev0, c->ev1);
     if (ms) *ms += t;
+    return SWB_OK;
+}
+
+// Packed batches at least this large may probe the candidates on their own pairs.
+constexpr int64_t kTuneMinPairs = 16384;
+
+// Rows per lane of the packed pass over `ppos`: SWB_BATCH16_R (8 or 14), else
+// the autotuner's recorded choice for the batch's bucket, else timed probes:
+// candidate i scores the pairs at indices i, i + 8, i + 16, ... of ppos (an
+// eighth of the batch each, the same length mix), those results are kept and
+// their positions leave ppos, and the candidate with the most cells per ms is
+// recorded.  Batches below kTuneMinPairs take kBatch16R.
+int tune_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &info,
+                const std::vector<int64_t> &order, std::vector<int64_t> &ppos, uint32_t flags,
+                std::vector<BestRec> &pbest, std::vector<int64_t> &redo, float *ms, int32_t *launches, int *R,
+                const char **how) {
+    *R = kBatch16R;
+    *how = "default";
+    if (const char *v = std::getenv("SWB_BATCH16_R")) {
+        const int r = std::atoi(v);
+        if (r == kBatch16R || r == kBatch16RShort) {
+            *R = r;
+            *how = "SWB_BATCH16_R";
+            return SWB_OK;
+        }
+    }
+    if (ppos.empty()) return SWB_OK;
+    // cells-weighted median rows and columns of the packed pairs
+    auto median = [&](bool rows) {
+        std::vector<std::pair<int64_t, double>> v;
+        v.reserve(ppos.size());
+        double total = 0.0;
+        for (int64_t k : ppos) {
+            const PairInfo &p = info[(size_t)order[(size_t)k]];
+            const double cells = (double)p.m * (double)p.n;
+            v.emplace_back(rows ? p.m : p.n, cells);
+            total += cells;
+        }
+        std::sort(v.begin(), v.end());
+        double acc = 0.0;
+        for (const auto &x : v)
+            if ((acc += x.second) >= 0.5 * total) return x.first;
+        return v.back().first;
+    };
+    const std::string key = batch_tune_key(c->sms, "batch16", median(true), median(false));
+    int cached = 0;
+    if (tune_lookup(key, &cached) && (cached == kBatch16R || cached == kBatch16RShort)) {
+        *R = cached;
+        *how = "cached";
+        return SWB_OK;
+    }
+    if ((int64_t)ppos.size() < kTuneMinPairs) return SWB_OK;
+    const int cands[2] = {kBatch16R, kBatch16RShort};
+    double rate[2] = {0.0, 0.0};
+    for (int i = 0; i < 2; ++i) {
+        std::vector<int64_t> sample;
+        double cells = 0.0;
+        for (size_t q = (size_t)i; q < ppos.size(); q += 8) {
+            sample.push_back(ppos[q]);
+            const PairInfo &p = info[(size_t)order[(size_t)ppos[q]]];
+            cells += (double)p.m * (double)p.n;
+        }
+        float t = 0.f;
+        const int rc = run_packed(c, base, info, order, sample, flags, cands[i], pbest, redo, &t);
+        if (rc != SWB_OK) return rc;
+        *launches += 2;
+        if (ms) *ms += t;
+        rate[i] = t > 0.f ? cells / (double)t : 0.0;
+    }
+    std::vector<int64_t> rest;
+    rest.reserve(ppos.size());
+    for (size_t q = 0; q < ppos.size(); ++q)
+        if (q % 8 >= 2) rest.push_back(ppos[q]);
+    ppos.swap(rest);
+    *R = rate[1] > rate[0] ? cands[1] : cands[0];
+    *how = "probed";
+    tune_record(key, *R);
     return SWB_OK;
 }
 
@@ -807,9 +885,16 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
             else rest.push_back((int64_t)k);
         }
         pbest.assign(order.size(), BestRec{});
-        int rc = run_packed(c, base, info, order, ppos, flags, pbest, rest, &ms1);
+        int Rp = kBatch16R;
+        const char *how = "";
+        int rc = tune_packed(c, base, info, order, ppos, flags, pbest, rest, &ms1, &launches, &Rp, &how);
         if (rc != SWB_OK) return rc;
-        launches += 2;
+        if (ph.on) std::fprintf(stderr, "swb batch: packed rows per lane %d (%s)\n", Rp, how);
+        if (!ppos.empty()) {
+            rc = run_packed(c, base, info, order, ppos, flags, Rp, pbest, rest, &ms1);
+            if (rc != SWB_OK) return rc;
+            launches += 2;
+        }
         ph.mark("packed pass");
         if (!rest.empty()) {
             std::vector<int64_t> sub(rest.size());

@@ -128,4 +128,11 @@ cudaError_t ctx_put(swb_ctx *c, void *dev_dst, const void *src, size_t bytes);
 int autotune_rows_per_lane(swb_ctx *c, const Stage1Args &base, bool tab, bool stores, int fallback,
                            bool strip_rows = false, int64_t sr_interval = 0);
 
+// The autotuner's table for batched passes: the bucket key of a pass over pairs
+// whose cells-weighted median is m rows by n columns, a cached choice for it
+// (also read from SWB_AUTOTUNE_CACHE) and the recording of a new one.
+std::string batch_tune_key(int sms, const char *pass, int64_t m, int64_t n);
+bool tune_lookup(const std::string &key, int *R);
+void tune_record(const std::string &key, int R);
+
 }  // namespace swb

@@ -1,5 +1,6 @@
 """One process of tests/test_autotune_gpu.py: aligns a seeded pair large enough
-for the autotuner (score only) and prints the result as JSON."""
+for the autotuner (score only), or with "batch" the seeded 20,000-pair batch
+(packed pass, log on stderr), and prints the result as JSON."""
 import json
 import os
 import random
@@ -20,7 +21,21 @@ def pair():
     return a, bytes(core)
 
 
-if __name__ == "__main__":
+def batch():
+    import numpy as np
+    from swb200 import synth
+    buf, refs, sc = synth.batched(BATCH_PAIRS, seed_extra=5)
+    with swb200.Context(device=0, verbose=1) as ctx:
+        r = ctx.batch_align(buf.tobytes(), refs, swb200.scoring(*sc), 0, trace_frac=0.0)
+    print(json.dumps({"score": np.asarray(r.score).tolist(), "end_row": np.asarray(r.end_row).tolist(),
+                      "end_col": np.asarray(r.end_col).tolist()}))
+
+
+BATCH_PAIRS = 20_000
+
+if __name__ == "__main__" and len(sys.argv) > 1 and sys.argv[1] == "batch":
+    batch()
+elif __name__ == "__main__":
     a, b = pair()
     with swb200.Context(device=0) as ctx:
         r = ctx.align(a, b, swb200.scoring(1, -3, -5, -2), swb200.FLAG_SCORE_ONLY)

@@ -2,10 +2,13 @@
 probes per shape bucket and kept in the file named by SWB_AUTOTUNE_CACHE.  The
 reference hard-wires its launch shape (src/SWutils.cpp:233-253).  A first
 process probes and appends the bucket's choice to the file; a second process
-reads it back and appends nothing; every candidate gives the same result."""
+reads it back and appends nothing; every candidate gives the same result.
+The packed batch pass is tuned the same way (448- or 256-row strips), its
+probes timed on strided samples of the batch's own pairs."""
 import json
 import os
 import random
+import re
 import subprocess
 import sys
 
@@ -55,3 +58,48 @@ def test_every_rows_per_lane_candidate_gives_the_same_result(gpu_ctx, monkeypatc
         for flags in (swb200.FLAG_SCORE_ONLY, 0):
             r = gpu_ctx.align(a, b, swb200.scoring(1, -3, -5, -2), flags)
             assert (r.score, r.end_row, r.end_col) == (e.score, e.row, e.col), (R, flags)
+
+
+def _run_batch(env):
+    p = subprocess.run([sys.executable, os.path.join(HERE, "autotune_worker.py"), "batch"], env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stdout + p.stderr
+    m = re.search(r"packed rows per lane (\d+) \((\w+)\)", p.stderr)
+    assert m, p.stderr
+    return json.loads(p.stdout.strip().splitlines()[-1]), int(m.group(1)), m.group(2)
+
+
+def test_batch_autotune_probes_once_and_the_cache_file_round_trips(tmp_path):
+    """A first process probes both strip heights on samples of the 20,000-pair
+    batch and records the bucket's choice; a second reads it and probes
+    nothing; a choice written by hand is used; every run gives the same
+    results, which equal the oracle's on a sample."""
+    cache = str(tmp_path / "autotune.txt")
+    env = {k: v for k, v in os.environ.items() if k not in ("SWB_BATCH16_R", "SWB_BATCH_PACK")}
+    env["SWB_AUTOTUNE_CACHE"] = cache
+    first, R1, how1 = _run_batch(env)
+    assert how1 == "probed" and R1 in (8, 14)
+    lines = open(cache).read().splitlines()
+    assert len(lines) == 1 and " batch16 tab " in lines[0], lines
+    key, R = lines[0].rsplit(" ", 1)
+    assert int(R) == R1
+    second, R2, how2 = _run_batch(env)
+    assert (R2, how2) == (R1, "cached")
+    assert open(cache).read().splitlines() == lines
+    assert second == first
+    other = 8 if R1 == 14 else 14
+    with open(cache, "w") as f:
+        f.write(f"{key} {other}\n")
+    third, R3, how3 = _run_batch(env)
+    assert (R3, how3) == (other, "cached")
+    assert third == first
+    # a sample against the oracle
+    import autotune_worker as W
+    from swb200 import synth
+    buf, refs, sc = synth.batched(W.BATCH_PAIRS, seed_extra=5)
+    buf = buf.tobytes()
+    for i in random.Random(2).sample(range(W.BATCH_PAIRS), 30):
+        qo, ql, to, tl = (int(x) for x in refs[i])
+        rows, cols, _ = O.orient(buf[qo:qo + ql], buf[to:to + tl])
+        e = O.stage1(rows, cols, O.scoring(*sc), O.TEXTBOOK, O.TIE_REFERENCE)
+        assert (first["score"][i], first["end_row"][i], first["end_col"][i]) == (e.score, e.row, e.col), i
