@@ -11,6 +11,7 @@
 #include <cstring>
 #include <numeric>
 #include <thread>
+#include <utility>
 #include <vector>
 
 #include "batch.h"
@@ -28,9 +29,11 @@ struct PairInfo {
 
 // Lays out the units of `order` (indices into info, already sorted) as one
 // launch: unit0 / ufirst / ucount / hbuf offsets; returns the unit count.
+// extent (optional, one per entry of order): compute only the top-left
+// rows x cols of the pair; the tie rule keeps the whole pair's geometry.
 int64_t layout_units(const std::vector<PairInfo> &info, const std::vector<int64_t> &order, uint32_t flags,
                      int strip_rows, std::vector<BatchPair> &bp, std::vector<int32_t> &unit_pair,
-                     int64_t *hbuf_entries) {
+                     int64_t *hbuf_entries, const std::vector<std::pair<int64_t, int64_t>> *extent = nullptr) {
     bp.resize(order.size());
     unit_pair.clear();
     int64_t units = 0, hb = 0;
@@ -40,9 +43,10 @@ int64_t layout_units(const std::vector<PairInfo> &info, const std::vector<int64_
         std::memset(&d, 0, sizeof d);
         d.row_off = p.row_off;
         d.col_off = p.col_off;
-        d.m = (int32_t)p.m;
-        d.n = (int32_t)p.n;
-        d.nstrips = (int32_t)((p.m + strip_rows - 1) / strip_rows);
+        const int64_t em = extent ? (*extent)[k].first : p.m, en = extent ? (*extent)[k].second : p.n;
+        d.m = (int32_t)em;
+        d.n = (int32_t)en;
+        d.nstrips = (int32_t)((em + strip_rows - 1) / strip_rows);
         d.unit0 = (int32_t)units;
         d.ufirst = (int32_t)units;
         d.ucount = d.nstrips;
@@ -51,7 +55,7 @@ int64_t layout_units(const std::vector<PairInfo> &info, const std::vector<int64_
         d.sc_every = 1 << 30;
         if (d.nstrips > 1) {
             d.hbuf_off = hb;
-            hb += p.n;
+            hb += en;
         }
         int32_t G = 0, T = 0;
         int64_t P1 = 0, P2 = 0;
@@ -967,10 +971,16 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
             for (size_t k = 0; k < tr.size(); ++k) bpw[k] = bp[(size_t)pos[(size_t)tr[k]]];
         } else if (!tr.empty()) {
             // store pass over the traced pairs: special rows every 512 rows (every
-            // strip), special columns every 256 columns
+            // strip), special columns every 256 columns.  The path ends at the end
+            // cell, and no cell below or right of it feeds a cell above and left
+            // of it, so only rows 0..end_row and columns 0..end_col are computed
+            // (their values and the best cell's tie key are the whole pair's).
             std::vector<int32_t> up2;
             int64_t hb2 = 0;
-            layout_units(info, tr, flags, kBatchStripRows, bpw, up2, &hb2);
+            std::vector<std::pair<int64_t, int64_t>> ext(tr.size());
+            for (size_t k = 0; k < tr.size(); ++k)
+                ext[k] = {out->items[tr[k]].end_row + 1, out->items[tr[k]].end_col + 1};
+            layout_units(info, tr, flags, kBatchStripRows, bpw, up2, &hb2, &ext);
             layout_stores(bpw, out->items, tr, &srn, &scn, &ops_total, &xp_total);
             int rc = ensure_stores(srn, scn);
             if (rc != SWB_OK) return rc;
