@@ -306,7 +306,7 @@ typedef struct {
     uint64_t hbm_budget_bytes;  /* admission budget (sequences + special rows/columns); 0 = 64 GiB */
     int64_t  long_cells;        /* rows * cols above which a request runs in the long lane; 0 = 2^32 */
     int32_t  max_batch;         /* most short requests per iteration; 0 = 8192                   */
-    int32_t  reserve_sms;       /* SMs kept for short iterations while a long request runs; 0 = 16 */
+    int32_t  reserve_sms;       /* SMs kept for short iterations while a long request runs; 0 = 4  */
     uint32_t flags;             /* SWB_FLAG_TIE_ROWMAJOR                                          */
 } swb_server_options;
 

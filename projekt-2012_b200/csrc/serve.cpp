@@ -282,7 +282,7 @@ int swb_server_create(const swb_server_options *opts, const swb_scoring *sc, swb
     if (s->o.hbm_budget_bytes == 0) s->o.hbm_budget_bytes = 64ULL << 30;
     if (s->o.long_cells <= 0) s->o.long_cells = 1LL << 32;
     if (s->o.max_batch <= 0) s->o.max_batch = 8192;
-    if (s->o.reserve_sms <= 0) s->o.reserve_sms = 16;
+    if (s->o.reserve_sms <= 0) s->o.reserve_sms = 4;  // 16 left short p99 the same and the long lane 4.5% slower
     s->sc = *sc;
     s->long_store_budget = s->o.hbm_budget_bytes / 2;
     swb_options co;
