@@ -213,8 +213,10 @@ int swb_score_block_device(swb_ctx *ctx, const void *d_rows, int64_t rows, const
  * result; the kernel's scratch is a fixed array inside this library (about
  * 16.1 MiB per device that loads it, held until exit).  Limits: cols <=
  * SWB_NOALLOC_MAX_COLS, rows <= SWB_NOALLOC_MAX_ROWS, else SWB_EUNSUPPORTED.
- * The first call on a device looks up the array's device address; make it
- * before any stream capture.  That first call also loads the array's module, which
+ * The call cannot be captured into a CUDA graph (it copies its result to the
+ * host and waits): on a stream that is capturing it returns SWB_EINVAL and
+ * leaves the capture intact.  The first call on a device looks up the array's
+ * device address.  That first call also loads the array's module, which
  * commits its memory and can fail with SWB_ECUDA (out of memory): callers that must
  * not fail later make it at start-up, where a call with rows = cols = 0 does only
  * this set-up.  The address is kept for the process: after a cudaDeviceReset of

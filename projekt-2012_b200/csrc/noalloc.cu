@@ -89,6 +89,15 @@ extern "C" int swb_score_pair_noalloc(int32_t device, const void *d_rows, int64_
         }
     } restore{prev};
 
+    // the call copies its result to the host and waits, which a stream capture
+    // cannot record: refuse it on a capturing stream rather than break the capture
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        const cudaError_t ce = cudaStreamIsCapturing((cudaStream_t)(uintptr_t)cuda_stream, &cs);
+        if (ce != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+            return noalloc_fail(SWB_EINVAL, "swb_score_pair_noalloc: the stream is capturing a graph");
+    }
+
     unsigned char *base = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_setup_mu);

@@ -112,3 +112,31 @@ def test_noalloc_set_up_call_with_empty_pair():
     rc = fn(0, None, 0, None, 0, C.byref(sc), 0, 0, C.byref(out))
     assert rc == swb200.SWB_OK, err()
     assert (out.score, out.end_row, out.end_col) == (0, 0, 0)
+
+
+def test_noalloc_refuses_a_capturing_stream_and_keeps_the_capture():
+    """On a stream that is capturing a graph the call returns SWB_EINVAL without
+    touching the stream; the capture ends normally and its graph replays."""
+    import torch
+    fn, err = _noalloc()
+    sc = swb200.scoring(1, -3, -5, -2)
+    r, c = _pair(5, 3000, 0.5)
+    tr = torch.frombuffer(bytearray(r), dtype=torch.uint8).cuda()
+    tc = torch.frombuffer(bytearray(c), dtype=torch.uint8).cuda()
+    x = torch.zeros(16, device="cuda")
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    rcs = []
+    with torch.cuda.graph(g, stream=s):
+        x.add_(1)
+        out = Score()
+        rcs.append(fn(0, tr.data_ptr(), len(r), tc.data_ptr(), len(c), C.byref(sc), 0, s.cuda_stream,
+                      C.byref(out)))
+    assert rcs == [swb200.SWB_EINVAL], err()
+    assert b"capturing" in err()
+    g.replay()
+    torch.cuda.synchronize()
+    assert float(x[0]) == 1.0
+    out = Score()   # outside the capture the same call works
+    assert fn(0, tr.data_ptr(), len(r), tc.data_ptr(), len(c), C.byref(sc), 0, s.cuda_stream, C.byref(out)) == 0
+    assert out.score > 0
