@@ -511,15 +511,19 @@ def main():
         if world > 1:
             dist.destroy_process_group()
         return
-    cpu = None if args.no_cpu_baseline else cpu_baseline(a, b, sc_t)
+    # the CPU baseline and the single-GPU sub-records (batched, serving, 10 Mbp
+    # pair) belong to the N = 1 line; at N > 1 they would hold every GPU for
+    # minutes while rank 0 alone works
+    single = world == 1
+    cpu = None if (args.no_cpu_baseline or not single) else cpu_baseline(a, b, sc_t)
     mixed_batched = mixed_serving = chrom = None
     ctx.close()
     del d_rows, d_cols, flush
     torch.cuda.empty_cache()
-    if not args.no_mixed:
+    if not args.no_mixed and single:
         mixed_batched = batched_metrics(args, local)
         mixed_serving = None if args.no_serving else serving_metrics(args, local)
-    if not args.no_chromosome and args.workload == "long":
+    if not args.no_chromosome and args.workload == "long" and single:
         chrom = chromosome_metrics(args, local, peak_cells["cells_per_s"])
     d2h = 64 + first.n_ops + 24 * len(first.xpoints)
     line = {
