@@ -311,15 +311,13 @@ __device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const D &dir, co
             const bool ok = in && (v & 3) == SRC_DIAG && !(v & BIT_DZERO);
             const uint32_t bal = __ballot_sync(0xffffffffu, ok);
             const int nrun = (bal == 0xffffffffu) ? 32 : __ffs(~bal) - 1;
-            int32_t s = 0;
-            if (lane < nrun) s = sg->rb[rr - R0] == sg->cb[cc - C0] ? a.match : a.mismatch;
-            // inclusive prefix of s over lanes: suffix after lane i's cell
-            int32_t ps = s;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int32_t u = __shfl_up_sync(0xffffffffu, ps, o);
-                if (lane >= o) ps += u;
-            }
+            // inclusive prefix over lanes of the run's substitution scores (the
+            // suffix after lane i's cell), from one ballot of the matching cells
+            const bool mt = lane < nrun && sg->rb[rr - R0] == sg->cb[cc - C0];
+            const uint32_t mb = __ballot_sync(0xffffffffu, mt);
+            const int nle = min(lane + 1, nrun);
+            const int mle = __popc(mb & (0xffffffffu >> (31 - lane)));
+            const int32_t ps = mle * a.match + (nle - mle) * a.mismatch;
             // crosspoint: moving from (rr, cc) to (rr-1, cc-1) enters row rr-1 from below
             const bool xp = lane < nrun && ((rr - 1 + 1) % X) == 0 && rr - 1 >= 0;
             const uint32_t xbal = __ballot_sync(0xffffffffu, xp);
@@ -334,7 +332,7 @@ __device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const D &dir, co
                 }
             }
             if (lane < nrun && nops + lane < a.ops_cap) a.ops[nops + lane] = 'M';
-            const int32_t tot = __shfl_sync(0xffffffffu, ps, 31);
+            const int32_t tot = __popc(mb) * a.match + (nrun - __popc(mb)) * a.mismatch;
             nops += nrun;
             suffix += tot;
             nxp += __popc(xbal);
@@ -488,9 +486,29 @@ __global__ void __launch_bounds__(kThreads) precompute_kernel(WalkArgs a, const 
 }
 
 // Sequence bytes of a block for the walk's diagonal scores.
+// The block's row and column bytes into shared memory by one warp: every load
+// of a lane is issued before its first store, so the warp waits for one round
+// trip to memory instead of one per 32 bytes (24 of them for a 512 x 256 block).
 __device__ void stage_bytes(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0, int64_t C1, Stage *s) {
-    for (int64_t j = threadIdx.x; j <= C1 - C0; j += blockDim.x) s->cb[j] = a.cols[C0 + j];
-    for (int64_t i = threadIdx.x; i <= R1 - R0; i += blockDim.x) s->rb[i] = a.rows[R0 + i];
+    const int lane = threadIdx.x & 31;
+    const int64_t h = R1 - R0 + 1, w = C1 - C0 + 1;  // h <= kBR, w <= kBC
+    uint8_t rv[kBR / 32], cv[kBC / 32];
+#pragma unroll
+    for (int u = 0; u < kBR / 32; ++u) {
+        const int64_t i = lane + 32 * u;
+        rv[u] = i < h ? __ldg(a.rows + R0 + i) : (uint8_t)0;
+    }
+#pragma unroll
+    for (int u = 0; u < kBC / 32; ++u) {
+        const int64_t j = lane + 32 * u;
+        cv[u] = j < w ? __ldg(a.cols + C0 + j) : (uint8_t)0;
+    }
+#pragma unroll
+    for (int u = 0; u < kBR / 32; ++u)
+        if (lane + 32 * u < h) s->rb[lane + 32 * u] = rv[u];
+#pragma unroll
+    for (int u = 0; u < kBC / 32; ++u)
+        if (lane + 32 * u < w) s->cb[lane + 32 * u] = cv[u];
 }
 
 // One warp walks the path through precomputed blocks: block (bi, bj) of the
