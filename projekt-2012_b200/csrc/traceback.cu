@@ -48,7 +48,13 @@ constexpr int kBC = 256;          // block columns (= special-column spacing)
 constexpr int kThreads = 128;     // recompute threads
 constexpr int kRT = kBR / kThreads;  // rows per recompute thread (4)
 
-enum : uint8_t { SRC_ZERO = 0, SRC_DIAG = 1, SRC_E = 2, SRC_F = 3, BIT_EEXT = 4, BIT_FEXT = 8, BIT_DZERO = 16 };
+// Direction byte of a cell: where H comes from (2 bits), whether E and F extend,
+// whether the diagonal predecessor's H is 0, and whether the cell's two bases
+// match (the walk takes the path's substitution scores from it, so it needs
+// no sequence bytes).
+enum : uint8_t {
+    SRC_ZERO = 0, SRC_DIAG = 1, SRC_E = 2, SRC_F = 3, BIT_EEXT = 4, BIT_FEXT = 8, BIT_DZERO = 16, BIT_MATCH = 32
+};
 enum : int32_t { ST_H = 0, ST_E = 1, ST_F = 2 };
 
 struct WalkArgs {
@@ -83,7 +89,7 @@ __device__ __forceinline__ int2 top_hf(const WalkArgs &a, int64_t R0, int64_t c)
         if (c < a.cc0) return make_int2((a.rtop && a.rleft) ? a.rtop[-1].x : 0, 0);  // the corner
         return a.rtop ? a.rtop[c - a.cc0] : make_int2(0, 0);
     }
-    const int64_t q = (R0 - a.rr0) / a.br - 1;
+    const int64_t q = (int32_t)(R0 - a.rr0) / a.br - 1;
     if (c < a.cc0) return make_int2(a.rleft ? a.rleft[R0 - 1 - a.rr0].x : 0, 0);
     return a.srows[q * (a.cc1 - a.cc0) + (c - a.cc0)];
 }
@@ -259,9 +265,11 @@ __device__ void recompute(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0,
                     const int32_t eext = El[i] + a.ext, eopen = Hl[i] + a.open;
                     const int32_t fext = fu + a.ext, fopen = hu + a.open;
                     const int32_t e = max(eext, eopen), f = max(fext, fopen);
-                    const int32_t dg = hd + (ra[i] == cb ? a.match : a.mismatch);
+                    const bool same = ra[i] == cb;
+                    const int32_t dg = hd + (same ? a.match : a.mismatch);
                     const int32_t hv = max(max(0, e), max(f, dg));
                     uint32_t v = hv == 0 ? SRC_ZERO : (hv == dg ? SRC_DIAG : (hv == e ? SRC_E : SRC_F));
+                    if (same) v |= BIT_MATCH;
                     if (eext == e) v |= BIT_EEXT;
                     if (fext == f) v |= BIT_FEXT;
                     if (hd == 0) v |= BIT_DZERO;
@@ -294,8 +302,10 @@ __device__ void recompute(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0,
 }
 
 // Warp 0 walks the path through the block [R0, R1] x [C0, C1].
+// Row and column indices fit 32 bits (pairs are limited to 2^31 - 64 rows), so
+// the crosspoint tests use 32-bit remainders.
 template <class D>
-__device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const D &dir, const Stage *sg, int64_t *S) {
+__device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const D &dir, int64_t *S) {
     const int lane = threadIdx.x & 31;
     int64_t r = S[kStR], c = S[kStC];
     int32_t state = (int32_t)S[kStState];
@@ -313,13 +323,13 @@ __device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const D &dir, co
             const int nrun = (bal == 0xffffffffu) ? 32 : __ffs(~bal) - 1;
             // inclusive prefix over lanes of the run's substitution scores (the
             // suffix after lane i's cell), from one ballot of the matching cells
-            const bool mt = lane < nrun && sg->rb[rr - R0] == sg->cb[cc - C0];
+            const bool mt = lane < nrun && (v & BIT_MATCH);
             const uint32_t mb = __ballot_sync(0xffffffffu, mt);
             const int nle = min(lane + 1, nrun);
             const int mle = __popc(mb & (0xffffffffu >> (31 - lane)));
             const int32_t ps = mle * a.match + (nle - mle) * a.mismatch;
             // crosspoint: moving from (rr, cc) to (rr-1, cc-1) enters row rr-1 from below
-            const bool xp = lane < nrun && ((rr - 1 + 1) % X) == 0 && rr - 1 >= 0;
+            const bool xp = lane < nrun && rr - 1 >= 0 && ((int32_t)rr % X) == 0;
             const uint32_t xbal = __ballot_sync(0xffffffffu, xp);
             if (xp) {
                 const int64_t slot = nxp + __popc(xbal & ((1u << lane) - 1));
@@ -344,7 +354,7 @@ __device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const D &dir, co
                 if (src == SRC_DIAG) {  // the start cell
                     if (lane == 0 && nops < a.ops_cap) a.ops[nops] = 'M';
                     nops += 1;
-                    suffix += sg->rb[r - R0] == sg->cb[c - C0] ? a.match : a.mismatch;
+                    suffix += (w & BIT_MATCH) ? a.match : a.mismatch;
                     S[kStStartR] = r;
                     S[kStStartC] = c;
                     done = true;
@@ -401,7 +411,7 @@ __device__ void walk(const WalkArgs &a, int64_t R0, int64_t C0, const D &dir, co
             const int64_t cost_i = (int64_t)(lane + 1) * a.ext + ((opened && lane == nrun - 1) ? a.open - a.ext : 0);
             // crosspoint: moving from (rr, c) up to (rr-1, c) enters row rr-1 from below;
             // the cell above is in F if this move extended the gap, else in H
-            const bool xp = lane < nrun && (rr % X) == 0 && rr - 1 >= 0;
+            const bool xp = lane < nrun && rr - 1 >= 0 && ((int32_t)rr % X) == 0;
             const uint32_t xbal = __ballot_sync(0xffffffffu, xp);
             if (xp) {
                 const int64_t slot = nxp + __popc(xbal & ((1u << lane) - 1));
@@ -444,7 +454,7 @@ __device__ void walk_body(const WalkArgs &a, const D &dir, Xchg *xc, Stage *sg, 
     for (; guard < (1 << 30); ++guard) {
         const int64_t r = S[kStR], c = S[kStC];
         if (S[kStDone] || S[kStErr] || r < a.rr0 || c < a.cc0) break;
-        const int64_t R0 = a.rr0 + ((r - a.rr0) / a.br) * a.br;
+        const int64_t R0 = a.rr0 + (int64_t)((int32_t)(r - a.rr0) / a.br) * a.br;
         const int64_t C0 = a.cc0 + ((c - a.cc0) / kBC) * kBC;
         stage_block(a, R0, r, C0, c, sg);
         __syncthreads();
@@ -455,7 +465,7 @@ __device__ void walk_body(const WalkArgs &a, const D &dir, Xchg *xc, Stage *sg, 
             __syncthreads();
             break;
         }
-        if (threadIdx.x < 32) walk(a, R0, C0, dir, sg, S);
+        if (threadIdx.x < 32) walk(a, R0, C0, dir, S);
         __syncthreads();
     }
     if (threadIdx.x < kStN) a.st[threadIdx.x] = S[threadIdx.x];
@@ -486,31 +496,6 @@ __global__ void __launch_bounds__(kThreads) precompute_kernel(WalkArgs a, const 
 }
 
 // Sequence bytes of a block for the walk's diagonal scores.
-// The block's row and column bytes into shared memory by one warp: every load
-// of a lane is issued before its first store, so the warp waits for one round
-// trip to memory instead of one per 32 bytes (24 of them for a 512 x 256 block).
-__device__ void stage_bytes(const WalkArgs &a, int64_t R0, int64_t R1, int64_t C0, int64_t C1, Stage *s) {
-    const int lane = threadIdx.x & 31;
-    const int64_t h = R1 - R0 + 1, w = C1 - C0 + 1;  // h <= kBR, w <= kBC
-    uint8_t rv[kBR / 32], cv[kBC / 32];
-#pragma unroll
-    for (int u = 0; u < kBR / 32; ++u) {
-        const int64_t i = lane + 32 * u;
-        rv[u] = i < h ? __ldg(a.rows + R0 + i) : (uint8_t)0;
-    }
-#pragma unroll
-    for (int u = 0; u < kBC / 32; ++u) {
-        const int64_t j = lane + 32 * u;
-        cv[u] = j < w ? __ldg(a.cols + C0 + j) : (uint8_t)0;
-    }
-#pragma unroll
-    for (int u = 0; u < kBR / 32; ++u)
-        if (lane + 32 * u < h) s->rb[lane + 32 * u] = rv[u];
-#pragma unroll
-    for (int u = 0; u < kBC / 32; ++u)
-        if (lane + 32 * u < w) s->cb[lane + 32 * u] = cv[u];
-}
-
 // One warp walks the path through precomputed blocks: block (bi, bj) of the
 // region (relative to rr0, cc0) is slot map[(bi - bi0) * mw + (bj - bj0)] of
 // gdir, or absent (-1).  Stops where the path enters an absent block, at the
@@ -534,14 +519,13 @@ __device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
 // on entering a block the warp copies the part the path can still reach (the
 // 128-row chunks at or above the current row, the steps up to the current
 // column + 31) from gdir with one bulk asynchronous copy (cp.async.bulk, the
-// TMA engine) per chunk, completing on an mbarrier, while it stages the
-// block's sequence bytes; every step of the walk is then a shared-memory read
-// instead of a dependent L2 round trip.
+// TMA engine) per chunk, completing on an mbarrier; every step of the walk is
+// then a shared-memory read instead of a dependent L2 round trip.  The
+// direction bytes carry the match bit, so no sequence bytes are read.
 __global__ void __launch_bounds__(32) corridor_walk_kernel(WalkArgs a, const uint32_t *gdir, const int32_t *map,
                                                            int64_t bi0, int64_t bj0, int64_t mh, int64_t mw,
                                                            const int32_t *err) {
     extern __shared__ __align__(16) uint32_t dtile[];  // kBlockWords words
-    __shared__ Stage sg;
     __shared__ int64_t S[kStN];
     __shared__ __align__(8) uint64_t bar_mem;
     const int lane = threadIdx.x;
@@ -561,7 +545,8 @@ __global__ void __launch_bounds__(32) corridor_walk_kernel(WalkArgs a, const uin
     for (;;) {
         const int64_t r = S[kStR], c = S[kStC];
         if (S[kStDone] || S[kStErr] || r < a.rr0 || c < a.cc0) break;
-        const int64_t bi = (r - a.rr0) / a.br, bj = (c - a.cc0) / kBC;
+        // region offsets fit 32 bits: 32-bit division
+        const int64_t bi = (int32_t)(r - a.rr0) / a.br, bj = (c - a.cc0) / kBC;
         if (bi < bi0 || bi >= bi0 + mh || bj < bj0 || bj >= bj0 + mw) break;
         const int32_t slot = map[(bi - bi0) * mw + (bj - bj0)];
         if (slot < 0) break;
@@ -584,7 +569,6 @@ __global__ void __launch_bounds__(32) corridor_walk_kernel(WalkArgs a, const uin
                     : "memory");
         }
         in_flight = true;
-        stage_bytes(a, R0, r, C0, c, &sg);
         const bool ok = __all_sync(0xffffffffu, bar_wait(bar, phase & 1));
         if (!ok) {
             if (lane == 0) S[kStErr] = 1;
@@ -594,7 +578,7 @@ __global__ void __launch_bounds__(32) corridor_walk_kernel(WalkArgs a, const uin
         in_flight = false;
         ++phase;
         __syncwarp();
-        walk(a, R0, C0, SmemDir{dtile}, &sg, S);
+        walk(a, R0, C0, SmemDir{dtile}, S);
         __syncwarp();
     }
     // A copy still in flight after its wait ran out writes this CTA's shared
