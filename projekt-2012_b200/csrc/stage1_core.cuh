@@ -472,14 +472,20 @@ __device__ bool run_strip(const A &a, int4 *ring, int4 *stage, int lane, int32_t
         // lane l stores special column j = q*sc_every - 1 at step j + l: a chunk of
         // steps [k, k+kCH) needs the check when some (t + 1) mod sc_every < 32
         const bool sc_window = a.scols != nullptr && ((k + kCH) & (a.sc_every - 1)) < 32 + kCH;
-        // The pair kernel's score-only launches unroll the chunk; the batched
-        // kernel and launches with stores keep it rolled (measured on the 1 Mbp
-        // pair: unrolling saves 5-8% of the score-only time but costs the
-        // store-mode kernel 27% and the batched kernel about 50%).
+        // The pair kernel's score-only launches unroll the chunk fully, launches
+        // with stores by 4 outside the special-column windows, the batched
+        // score-only kernel not at all (measured on the 1 Mbp pair: the full
+        // unroll saves 5-8% of the score-only time but costs the store-mode
+        // kernel 20-27% and the batched kernel about 50%; unrolled by 4 the
+        // store-mode kernel is 5.4% faster than rolled, 563.8 vs 595.8 ms, and
+        // 1.9% on the 10 Mbp pair; by 2, 568.4 ms).
         if (STORES && sc_window) {
             for (int u = 0; u < kCH; ++u) step<R, TAB, false, true>(L, a, b, ring, stage, lane, sc, k + u);
         } else if constexpr (UNROLL) {
 #pragma unroll
+            for (int u = 0; u < kCH; ++u) step<R, TAB, false, false>(L, a, b, ring, stage, lane, sc, k + u);
+        } else if constexpr (STORES) {
+#pragma unroll 4
             for (int u = 0; u < kCH; ++u) step<R, TAB, false, false>(L, a, b, ring, stage, lane, sc, k + u);
         } else {
             for (int u = 0; u < kCH; ++u) step<R, TAB, false, false>(L, a, b, ring, stage, lane, sc, k + u);
