@@ -63,7 +63,9 @@ struct PackedPair {
     int64_t hbuf_off;                // first of the N hand-off entries (packs of more than one strip)
     int32_t m[2], n[2];              // m = n = 0: an empty half
     int32_t M, N;
-    int32_t unit0, nstrips;          // units [unit0, unit0 + nstrips) of this launch
+    int32_t unit0, nstrips;          // strip s keeps its two best records at ubest[2 (unit0 + s) + half]
+    int32_t item0, whole;            // work items: one (whole = 1: one warp runs every strip in turn)
+                                     // or one per strip, items [item0, item0 + nstrips)
     int32_t slot[2];                 // pbest / gbest / saturation slot of each half
     TieGeom tie[2];
 };
@@ -77,11 +79,11 @@ struct Batch16Args {
     uint32_t mm4;               // the table word of a column past a pair's end (a mismatch for every code)
     int32_t sat_lim;            // a half's column maximum (H + open) at or above this flags its pair
     const PackedPair *pairs;
-    const int32_t *unit_pair;   // work unit -> packed pair
-    int64_t nunits;
+    const int32_t *unit_pair;   // work item -> packed pair
+    int64_t nunits;             // work items
     int4 *hbuf;
     int32_t *gbest;             // per slot: best H seen so far
-    BestRec *ubest;             // per unit: two records (half 0, half 1)
+    BestRec *ubest;             // per strip of every packed pair: two records (half 0, half 1)
     int32_t *ctl;               // [0] unit counter, [1] error code, [2] abort flag
     int32_t *sat;               // per slot: 1 when the pair reached the 16-bit limit
     int64_t wait_limit;
@@ -93,6 +95,8 @@ constexpr int kBatch16R = 14;
 constexpr int kBatch16RShort = 8;
 
 cudaError_t batch16_configure();
+// Warps of a full packed launch (the grid batch16_launch uses at most).
+int batch16_resident_warps(int R, int sms, int max_blocks);
 // R: kBatch16R or kBatch16RShort; the packed pairs' strip counts must use it.
 cudaError_t batch16_launch(const Batch16Args &a, int R, int sms, int max_blocks, int64_t npacked, BestRec *pbest,
                            cudaStream_t st);

@@ -298,35 +298,45 @@ __global__ void __launch_bounds__(kWarps * 32, 4) batch16_kernel(Batch16Args g) 
         u = __shfl_sync(0xffffffffu, u, 0);
         if (u >= g.nunits || ld_volatile(&g.ctl[2]) != 0) break;
         const PackedPair d = g.pairs[g.unit_pair[u]];
-        Best ba, bb;
-        init_best(ba, g.open);
-        init_best(bb, g.open);
-        if (!run_strip16<R>(g, d, ring, stage, lane, u - d.unit0, &ba, &bb)) {
-            if (lane == 0) {
-                atomicCAS(&g.ctl[1], kErrNone, kErrTimeout);
-                atomicExch(&g.ctl[2], 1);
+        // a whole pair: every strip in turn (the strip above is always complete,
+        // so no wait ends up spinning); else the item's one strip
+        const int32_t s0 = d.whole ? 0 : u - d.item0, s1 = d.whole ? d.nstrips : s0 + 1;
+        bool ok = true;
+        for (int32_t s = s0; s < s1 && ok; ++s) {
+            Best ba, bb;
+            init_best(ba, g.open);
+            init_best(bb, g.open);
+            if (!run_strip16<R>(g, d, ring, stage, lane, s, &ba, &bb)) {
+                if (lane == 0) {
+                    atomicCAS(&g.ctl[1], kErrNone, kErrTimeout);
+                    atomicExch(&g.ctl[2], 1);
+                }
+                ok = false;
+                break;
             }
-            break;
+            key_best(&ba, d.tie[0], 0, 0);
+            key_best(&bb, d.tie[1], 0, 0);
+            warp_best(ba);
+            warp_best(bb);
+            if (lane == 0) {
+                const int64_t ub = 2 * ((int64_t)d.unit0 + s);
+                BestRec r;
+                r.ho = ba.ho;
+                r.valid = (ba.key != ~0ULL) ? 1 : 0;
+                r.key = ba.key;
+                r.row = ba.row;
+                r.col = ba.col;
+                g.ubest[ub] = r;
+                r.ho = bb.ho;
+                r.valid = (bb.key != ~0ULL) ? 1 : 0;
+                r.key = bb.key;
+                r.row = bb.row;
+                r.col = bb.col;
+                g.ubest[ub + 1] = r;
+            }
+            __syncwarp();
         }
-        key_best(&ba, d.tie[0], 0, 0);
-        key_best(&bb, d.tie[1], 0, 0);
-        warp_best(ba);
-        warp_best(bb);
-        if (lane == 0) {
-            BestRec r;
-            r.ho = ba.ho;
-            r.valid = (ba.key != ~0ULL) ? 1 : 0;
-            r.key = ba.key;
-            r.row = ba.row;
-            r.col = ba.col;
-            g.ubest[2 * (int64_t)u] = r;
-            r.ho = bb.ho;
-            r.valid = (bb.key != ~0ULL) ? 1 : 0;
-            r.key = bb.key;
-            r.row = bb.row;
-            r.col = bb.col;
-            g.ubest[2 * (int64_t)u + 1] = r;
-        }
+        if (!ok) break;
     }
 }
 
@@ -379,6 +389,13 @@ cudaError_t batch16_configure() {
     cudaError_t e1 = cudaFuncSetAttribute((const void *)batch16_kernel<kBatch16RShort>, A, c);
     cudaError_t e2 = cudaFuncSetAttribute((const void *)batch16_reduce_kernel, A, c);
     return e != cudaSuccess ? e : (e1 != cudaSuccess ? e1 : e2);
+}
+
+int batch16_resident_warps(int R, int sms, int max_blocks) {
+    const int per_sm = std::max(1, R == kBatch16R ? max_blocks16<kBatch16R>() : max_blocks16<kBatch16RShort>());
+    int64_t blocks = (int64_t)per_sm * sms;
+    if (max_blocks > 0 && max_blocks < blocks) blocks = max_blocks;
+    return (int)(blocks * kWarps);
 }
 
 cudaError_t batch16_launch(const Batch16Args &a, int R, int sms, int max_blocks, int64_t npacked, BestRec *pbest,

@@ -225,6 +225,21 @@ bool packing_enabled() {
 // it is packed without that risk.
 constexpr int32_t kSatLimit = 32767 - 256;
 
+// Which packed pairs run on one warp, strip after strip, instead of one strip
+// per warp chained through the hand-off buffer.  With far more pairs than
+// resident warps a short pair needs no pipeline across warps (whose strips
+// would each spin while the strip above gets ahead); a long one keeps it, so
+// that no single warp holds the batch's tail.  A pair runs whole when its
+// packed rectangle is at most a tenth of one warp's share of the launch's
+// cells: on the 100,000-pair batch that is about 8 strips of 448 rows
+// (packed kernel 195.4 -> 176.2 ms; whole up to 16 strips, 206.0 ms).
+// SWB_BATCH16_WHOLE=k instead runs pairs of at most k strips whole (0: none).
+constexpr int64_t kWholeShareDiv = 10;
+int32_t packed_whole_strips() {
+    if (const char *v = std::getenv("SWB_BATCH16_WHOLE")) return std::max(0, std::atoi(v));
+    return -1;
+}
+
 // The packed scoring pass over the positions `pos` of `order` with R rows per
 // lane: pairs sorted by strip count and width and taken two at a time (a pair
 // whose neighbour has another strip count gets an empty partner).  Fills
@@ -235,6 +250,7 @@ int run_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &i
                std::vector<BestRec> &pbest, std::vector<int64_t> &redo, float *ms) {
     cudaError_t e;
     const int64_t H = 32LL * R;
+    const int32_t whole_max = packed_whole_strips();  // -1: by the cell share
     auto strips = [&](int64_t k) { return (info[(size_t)order[(size_t)k]].m + H - 1) / H; };
     // strip count, then width, both descending
     sort_desc(pos, [&](int64_t x) {
@@ -279,12 +295,22 @@ int run_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &i
             d.hbuf_off = hb;
             hb += d.N;
         }
-        for (int32_t s = 0; s < d.nstrips; ++s) up.push_back((int32_t)pp.size());
         units += d.nstrips;
         pp.push_back(d);
     }
-    const int64_t np = (int64_t)pp.size(), nslots = (int64_t)order.size() + 1;
-    const size_t pp_bytes = sizeof(PackedPair) * (size_t)np, up_bytes = sizeof(int32_t) * (size_t)units;
+    // whole pairs and the work items (pairs stay in the order above)
+    double rect = 0.0;
+    for (const PackedPair &d : pp) rect += (double)d.M * (double)d.N;
+    const double share = rect / std::max(1, batch16_resident_warps(R, c->sms, c->max_blocks));
+    for (size_t q = 0; q < pp.size(); ++q) {
+        PackedPair &d = pp[q];
+        d.whole = whole_max >= 0 ? (d.nstrips <= whole_max ? 1 : 0)
+                                 : ((double)d.M * (double)d.N * (double)kWholeShareDiv <= share ? 1 : 0);
+        d.item0 = (int32_t)up.size();
+        for (int32_t s = 0; s < (d.whole ? 1 : d.nstrips); ++s) up.push_back((int32_t)q);
+    }
+    const int64_t np = (int64_t)pp.size(), nslots = (int64_t)order.size() + 1, items = (int64_t)up.size();
+    const size_t pp_bytes = sizeof(PackedPair) * (size_t)np, up_bytes = sizeof(int32_t) * (size_t)items;
     const size_t back = sizeof(BestRec) * (size_t)nslots + sizeof(int32_t) * (size_t)nslots + 64;
     if ((e = c->b_pairs.ensure(pp_bytes)) != cudaSuccess || (e = c->b_units.ensure(up_bytes)) != cudaSuccess ||
         (e = c->b_hbuf.ensure(sizeof(int4) * (size_t)std::max<int64_t>(1, hb))) != cudaSuccess ||
@@ -309,7 +335,7 @@ int run_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &i
     a.sat_lim = kSatLimit;
     a.pairs = (const PackedPair *)c->b_pairs.p;
     a.unit_pair = (const int32_t *)c->b_units.p;
-    a.nunits = units;
+    a.nunits = items;
     a.hbuf = (int4 *)c->b_hbuf.p;
     a.gbest = (int32_t *)c->b_gbest.p;
     a.ubest = (BestRec *)c->b_ubest.p;

@@ -214,15 +214,21 @@ def _packable_batch(seed, n, extra=()):
     return pairs
 
 
-@pytest.mark.parametrize("tie_flag,rows_per_lane", [(0, "14"), (swb200.FLAG_TIE_ROWMAJOR, "14"), (0, "8"),
-                                                    (swb200.FLAG_TIE_ROWMAJOR, "8")])
-def test_packed_16bit_pass_equals_int32_and_oracle(gpu_ctx, monkeypatch, tie_flag, rows_per_lane):
+RL = swb200.FLAG_TIE_ROWMAJOR
+
+
+@pytest.mark.parametrize("tie_flag,rows_per_lane,whole", [(0, "14", ""), (RL, "14", ""), (0, "8", ""), (RL, "8", ""),
+                                                          (0, "14", "64"), (RL, "8", "64"), (0, "14", "0")])
+def test_packed_16bit_pass_equals_int32_and_oracle(gpu_ctx, monkeypatch, tie_flag, rows_per_lane, whole):
     """A batch of >= 2,048 pairs in the table mode runs its scoring pass two pairs
-    per warp in packed 16-bit lanes (448- or 256-row strips); every pair gets
-    exactly the int32 pass's result (SWB_BATCH_PACK=0) and, on a sample, the
-    oracle's, under both tie rules; the traced pairs' store pass re-checks the
-    packed scores."""
+    per warp in packed 16-bit lanes (448- or 256-row strips; short pairs strip
+    after strip on one warp, long ones chained across warps, or all of them one
+    way with SWB_BATCH16_WHOLE); every pair gets exactly the int32 pass's result
+    (SWB_BATCH_PACK=0) and, on a sample, the oracle's, under both tie rules; the
+    traced pairs' store pass re-checks the packed scores."""
     monkeypatch.setenv("SWB_BATCH16_R", rows_per_lane)
+    if whole:
+        monkeypatch.setenv("SWB_BATCH16_WHOLE", whole)
     pairs = _packable_batch(21 + tie_flag, 2600, [(b"", b"ACGT"), (b"A" * 600, b"A" * 300)])
     buf, refs = _pack(pairs)
     sc = (2, -3, -5, -2)
@@ -241,13 +247,15 @@ def test_packed_16bit_pass_equals_int32_and_oracle(gpu_ctx, monkeypatch, tie_fla
         assert (packed.score[i], packed.end_row[i], packed.end_col[i], bool(packed.swapped[i])) == (s, r, c, sw), i
 
 
-@pytest.mark.parametrize("rows_per_lane", ["14", "8"])
-def test_packed_pass_detects_16bit_saturation_and_redoes_in_int32(gpu_ctx, monkeypatch, rows_per_lane):
+@pytest.mark.parametrize("rows_per_lane,whole", [("14", ""), ("8", ""), ("14", "64")])
+def test_packed_pass_detects_16bit_saturation_and_redoes_in_int32(gpu_ctx, monkeypatch, rows_per_lane, whole):
     """With the test flag every pair is packed, also identical pairs of 17,000 bp
     whose score (2 x 17,000 = 34,000) does not fit 16 bits: the kernel flags
     them when a column maximum reaches the limit and they are scored again in
     int32, so the results equal the int32 pass and the exact answer."""
     monkeypatch.setenv("SWB_BATCH16_R", rows_per_lane)
+    if whole:
+        monkeypatch.setenv("SWB_BATCH16_WHOLE", whole)
     rng = random.Random(77)
     longs = []
     for L in (17_000, 16_600):
