@@ -64,8 +64,8 @@ struct PackedPair {
     int32_t m[2], n[2];              // m = n = 0: an empty half
     int32_t M, N;
     int32_t unit0, nstrips;          // strip s keeps its two best records at ubest[2 (unit0 + s) + half]
-    int32_t item0, whole;            // work items: one (whole = 1: one warp runs every strip in turn)
-                                     // or one per strip, items [item0, item0 + nstrips)
+    int32_t whole, pad_;             // 1: one work item, one warp runs every strip in turn;
+                                     // 0: one work item per strip, chained across warps
     int32_t slot[2];                 // pbest / gbest / saturation slot of each half
     TieGeom tie[2];
 };
@@ -79,7 +79,7 @@ struct Batch16Args {
     uint32_t mm4;               // the table word of a column past a pair's end (a mismatch for every code)
     int32_t sat_lim;            // a half's column maximum (H + open) at or above this flags its pair
     const PackedPair *pairs;
-    const int32_t *unit_pair;   // work item -> packed pair
+    const int2 *items;          // work item -> (packed pair, strip); claimed in this order
     int64_t nunits;             // work items
     int4 *hbuf;
     int32_t *gbest;             // per slot: best H seen so far

@@ -297,10 +297,11 @@ __global__ void __launch_bounds__(kWarps * 32, 4) batch16_kernel(Batch16Args g) 
         if (lane == 0) u = atomicAdd(&g.ctl[0], 1);
         u = __shfl_sync(0xffffffffu, u, 0);
         if (u >= g.nunits || ld_volatile(&g.ctl[2]) != 0) break;
-        const PackedPair d = g.pairs[g.unit_pair[u]];
+        const int2 it = g.items[u];
+        const PackedPair d = g.pairs[it.x];
         // a whole pair: every strip in turn (the strip above is always complete,
         // so no wait ends up spinning); else the item's one strip
-        const int32_t s0 = d.whole ? 0 : u - d.item0, s1 = d.whole ? d.nstrips : s0 + 1;
+        const int32_t s0 = it.y, s1 = d.whole ? d.nstrips : s0 + 1;
         bool ok = true;
         for (int32_t s = s0; s < s1 && ok; ++s) {
             Best ba, bb;

@@ -258,7 +258,7 @@ int run_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &i
     });
     const int32_t dummy = (int32_t)order.size();  // slot of an empty half
     std::vector<PackedPair> pp;
-    std::vector<int32_t> up;
+    std::vector<int2> up;  // work items
     int64_t units = 0, hb = 0;
     for (size_t i = 0; i < pos.size();) {
         const int64_t ka = pos[i];
@@ -302,15 +302,42 @@ int run_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &i
     double rect = 0.0;
     for (const PackedPair &d : pp) rect += (double)d.M * (double)d.N;
     const double share = rect / std::max(1, batch16_resident_warps(R, c->sms, c->max_blocks));
+    std::vector<int32_t> chained;  // strip counts descending, as pp
     for (size_t q = 0; q < pp.size(); ++q) {
         PackedPair &d = pp[q];
         d.whole = whole_max >= 0 ? (d.nstrips <= whole_max ? 1 : 0)
                                  : ((double)d.M * (double)d.N * (double)kWholeShareDiv <= share ? 1 : 0);
-        d.item0 = (int32_t)up.size();
-        for (int32_t s = 0; s < (d.whole ? 1 : d.nstrips); ++s) up.push_back((int32_t)q);
+        if (!d.whole) chained.push_back((int32_t)q);
     }
+    // Claim order.  A chained pair's strip s waits until strip s - 1 is about
+    // kLagSteps steps ahead; claimed pair by pair, the warps that take strips
+    // 0..s of a pair start together and strip s spins s times that long (16% of
+    // the packed pass on the 100,000-pair batch).  So the chained pairs go
+    // strip-major (strip 0 of each, then strip 1, ...), and each strip is
+    // claimed long after the one above it.  A pair whose own chain (N columns
+    // plus the lag of every strip) is at least half of one warp's share of the
+    // launch would then finish late and hold the tail: those go first, pair by
+    // pair.  Whole pairs follow, largest first, and fill the tail.  Every strip
+    // is claimed after the strip it waits for.
+    constexpr double kLagSteps = 84.0;
+    const double share_steps = share / (double)H;
+    std::vector<int32_t> flow;  // non-critical chained pairs, strip counts descending
+    for (int32_t q : chained) {
+        const PackedPair &d = pp[(size_t)q];
+        if (2.0 * ((double)d.N + (d.nstrips - 1) * kLagSteps) >= share_steps)
+            for (int32_t s = 0; s < d.nstrips; ++s) up.push_back(make_int2(q, s));
+        else
+            flow.push_back(q);
+    }
+    // (pp is sorted by strip count, so the pairs of `flow` with more than s
+    // strips are a prefix of it)
+    for (int32_t s = 0; !flow.empty() && s < pp[(size_t)flow[0]].nstrips; ++s)
+        for (size_t i = 0; i < flow.size() && pp[(size_t)flow[i]].nstrips > s; ++i)
+            up.push_back(make_int2(flow[i], s));
+    for (size_t q = 0; q < pp.size(); ++q)
+        if (pp[q].whole) up.push_back(make_int2((int32_t)q, 0));
     const int64_t np = (int64_t)pp.size(), nslots = (int64_t)order.size() + 1, items = (int64_t)up.size();
-    const size_t pp_bytes = sizeof(PackedPair) * (size_t)np, up_bytes = sizeof(int32_t) * (size_t)items;
+    const size_t pp_bytes = sizeof(PackedPair) * (size_t)np, up_bytes = sizeof(int2) * (size_t)items;
     const size_t back = sizeof(BestRec) * (size_t)nslots + sizeof(int32_t) * (size_t)nslots + 64;
     if ((e = c->b_pairs.ensure(pp_bytes)) != cudaSuccess || (e = c->b_units.ensure(up_bytes)) != cudaSuccess ||
         (e = c->b_hbuf.ensure(sizeof(int4) * (size_t)std::max<int64_t>(1, hb))) != cudaSuccess ||
@@ -334,7 +361,7 @@ int run_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &i
     a.mm4 = base.tab_hi;
     a.sat_lim = kSatLimit;
     a.pairs = (const PackedPair *)c->b_pairs.p;
-    a.unit_pair = (const int32_t *)c->b_units.p;
+    a.items = (const int2 *)c->b_units.p;
     a.nunits = items;
     a.hbuf = (int4 *)c->b_hbuf.p;
     a.gbest = (int32_t *)c->b_gbest.p;
