@@ -130,7 +130,8 @@ __device__ __forceinline__ void batch_body(const BatchArgs &g) {
         Best b;
         init_best(b, g.open);
         int32_t bho = b.ho;
-        if (!run_strip<R, TAB, !std::is_same<S, NoStores>::value, false>(v, ring, stage, lane, u - d.unit0, &b, bho)) {
+        const int32_t strip = g.unit_strip ? g.unit_strip[u] : u - d.unit0;
+        if (!run_strip<R, TAB, !std::is_same<S, NoStores>::value, false>(v, ring, stage, lane, strip, &b, bho)) {
             if (lane == 0) {
                 atomicCAS(&g.ctl[1], kErrNone, kErrTimeout);
                 atomicExch(&g.ctl[2], 1);
@@ -158,7 +159,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs &g) {
             r.key = b.key;
             r.row = b.row;
             r.col = b.col;
-            g.ubest[u] = r;
+            g.ubest[d.ufirst + strip] = r;
         }
     }
 }
@@ -459,6 +460,12 @@ int batch_max_blocks_per_sm(bool tab, BatchMode mode) {
     if (mode == kBatchBounds) return tab ? max_blocks<16, true, WithBounds>() : max_blocks<16, false, WithBounds>();
     if (mode == kBatchStores) return tab ? max_blocks<16, true, WithStores>() : max_blocks<16, false, WithStores>();
     return tab ? max_blocks<16, true, NoStores>() : max_blocks<16, false, NoStores>();
+}
+
+int batch_resident_warps(bool tab, BatchMode mode, int sms, int max_blocks) {
+    int64_t blocks = (int64_t)std::max(1, batch_max_blocks_per_sm(tab, mode)) * sms;
+    if (max_blocks > 0 && max_blocks < blocks) blocks = max_blocks;
+    return (int)(blocks * kWarps);
 }
 
 cudaError_t batch_launch(const BatchArgs &a, bool tab, BatchMode mode, int R, int sms, int max_blocks, int64_t npairs,

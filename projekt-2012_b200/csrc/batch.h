@@ -45,11 +45,12 @@ struct BatchArgs {
     uint32_t tab_hi;
     const BatchPair *pairs;
     const int32_t *unit_pair;  // work unit -> index into pairs; units are claimed in this order
+    const int32_t *unit_strip; // if set, work unit -> strip of its pair; else the strip is u - unit0
     int64_t nunits;
     const int64_t *nunits_dev; // if set, the unit count is read here (graphed launches) instead
     int4 *hbuf;
     int32_t *gbest;            // per pair slot: best H seen so far
-    BestRec *ubest;            // per work unit: best cell of that strip
+    BestRec *ubest;            // per strip: best cell, at ufirst + strip of its pair
     int32_t *ctl;              // [0] unit counter, [1] error code, [2] abort flag
     int2 *srows, *scols;       // store pass: special rows (H, F) / columns (H, E) of every pair
     int64_t wait_limit;        // bound of each wait for the strip above, in SM clock cycles; 0 = default
@@ -157,6 +158,8 @@ cudaError_t batch_launch(const BatchArgs &a, bool tab, BatchMode mode, int R, in
 cudaError_t batch_encode(const uint8_t *seq, int64_t bytes, const uint8_t *d_lut, uint8_t *rcode, uint32_t *ctab,
                          int32_t mt1, int32_t mm1, uint32_t *tab_hi, cudaStream_t st);
 int batch_max_blocks_per_sm(bool tab, BatchMode mode);
+// Warps of a full batched launch of that mode (the grid batch_launch uses at most).
+int batch_resident_warps(bool tab, BatchMode mode, int sms, int max_blocks);
 // Rows per lane of score-only batched launches (16 unless SWB_BATCH_R overrides).
 int batch_score_rows_per_lane();
 

@@ -102,14 +102,59 @@ int64_t layout_units(const std::vector<PairInfo> &info, const std::vector<int64_
     return units;
 }
 
+// Claim order of a launch's strips: pairs whose own chain (n columns plus the
+// hand-off lag of every strip) is at least half of one warp's share of the
+// launch pair by pair, first; the others strip-major (strip 0 of each, then
+// strip 1, ...), so that a strip is seldom claimed before the strip above it is
+// far enough ahead.  Every strip comes after the one it waits for.  Appends
+// (pair, strip) to up / us; nstrips[k], n[k]: pair k's strips and columns.
+void claim_order(const std::vector<int32_t> &nstrips, const std::vector<int32_t> &n, double share_steps,
+                 std::vector<int32_t> &up, std::vector<int32_t> &us) {
+    constexpr double kLagSteps = 84.0;
+    std::vector<int32_t> flow;
+    for (size_t k = 0; k < nstrips.size(); ++k) {
+        if (2.0 * ((double)n[k] + (nstrips[k] - 1) * kLagSteps) >= share_steps) {
+            for (int32_t s = 0; s < nstrips[k]; ++s) {
+                up.push_back((int32_t)k);
+                us.push_back(s);
+            }
+        } else {
+            flow.push_back((int32_t)k);
+        }
+    }
+    std::stable_sort(flow.begin(), flow.end(), [&](int32_t x, int32_t y) { return nstrips[x] > nstrips[y]; });
+    for (int32_t s = 0; !flow.empty() && s < nstrips[(size_t)flow[0]]; ++s)
+        for (size_t i = 0; i < flow.size() && nstrips[(size_t)flow[i]] > s; ++i) {
+            up.push_back(flow[i]);
+            us.push_back(s);
+        }
+}
+
 // Runs one scoring launch (optionally the store pass) over bp; pbest receives
-// one record per entry of bp (slot k).
+// one record per entry of bp (slot k).  strip_major: claim the strips in
+// claim_order instead of pair by pair.
 int run_launch(swb_ctx *c, const uint8_t *d_seq, bool tab, const BatchArgs &base, std::vector<BatchPair> &bp,
                std::vector<int32_t> &unit_pair, int64_t hbuf_entries, bool stores, int R, std::vector<BestRec> &pbest,
-               float *ms) {
+               float *ms, bool strip_major = false) {
     cudaError_t e;
     const int64_t np = (int64_t)bp.size(), nu = (int64_t)unit_pair.size();
-    const size_t bp_bytes = sizeof(BatchPair) * (size_t)np, up_bytes = sizeof(int32_t) * (size_t)nu;
+    std::vector<int32_t> us;
+    if (strip_major && np > 0) {
+        std::vector<int32_t> ns((size_t)np), nc((size_t)np), up;
+        double rect = 0.0;
+        for (int64_t k = 0; k < np; ++k) {
+            ns[(size_t)k] = bp[(size_t)k].nstrips;
+            nc[(size_t)k] = bp[(size_t)k].n;
+            rect += (double)bp[(size_t)k].m * (double)bp[(size_t)k].n;
+        }
+        const int warps = std::max(1, batch_resident_warps(tab, stores ? kBatchStores : kBatchScore, c->sms,
+                                                          c->max_blocks));
+        up.reserve((size_t)nu);
+        us.reserve((size_t)nu);
+        claim_order(ns, nc, rect / warps / (32.0 * R), up, us);
+        unit_pair.swap(up);
+    }
+    const size_t bp_bytes = sizeof(BatchPair) * (size_t)np, up_bytes = sizeof(int32_t) * (size_t)nu * (us.empty() ? 1 : 2);
     if ((e = c->b_pairs.ensure(bp_bytes)) != cudaSuccess || (e = c->b_units.ensure(up_bytes)) != cudaSuccess ||
         (e = c->b_hbuf.ensure(sizeof(int4) * (size_t)std::max<int64_t>(1, hbuf_entries))) != cudaSuccess ||
         (e = c->b_gbest.ensure(sizeof(int32_t) * (size_t)np)) != cudaSuccess ||
@@ -121,12 +166,14 @@ int run_launch(swb_ctx *c, const uint8_t *d_seq, bool tab, const BatchArgs &base
     // descriptors through pinned staging (one buffer, two copies)
     uint8_t *hs = (uint8_t *)c->h_stage.p;
     std::memcpy(hs, bp.data(), bp_bytes);
-    std::memcpy(hs + bp_bytes, unit_pair.data(), up_bytes);
+    std::memcpy(hs + bp_bytes, unit_pair.data(), sizeof(int32_t) * (size_t)nu);
+    if (!us.empty()) std::memcpy(hs + bp_bytes + sizeof(int32_t) * (size_t)nu, us.data(), sizeof(int32_t) * (size_t)nu);
     BatchArgs a = base;
     a.seq = d_seq;
     a.cseq = d_seq;
     a.pairs = (const BatchPair *)c->b_pairs.p;
     a.unit_pair = (const int32_t *)c->b_units.p;
+    a.unit_strip = us.empty() ? nullptr : (const int32_t *)c->b_units.p + nu;
     a.nunits = nu;
     a.hbuf = (int4 *)c->b_hbuf.p;
     a.gbest = (int32_t *)c->b_gbest.p;
@@ -990,7 +1037,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
             std::vector<BestRec> pb2;
             int64_t hb2 = 0;
             layout_units(info, sub, flags, 32 * R1, bp2, up2, &hb2);
-            rc = run_launch(c, d_seq, tab, base, bp2, up2, hb2, false, R1, pb2, &ms1);
+            rc = run_launch(c, d_seq, tab, base, bp2, up2, hb2, false, R1, pb2, &ms1, true);
             if (rc != SWB_OK) return rc;
             launches += 2;
             for (size_t i = 0; i < rest.size(); ++i) pbest[(size_t)rest[i]] = pb2[i];
@@ -1004,7 +1051,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
             a1.srows = (int2 *)c->b_srows.p;
             a1.scols = (int2 *)c->b_scols.p;
         }
-        int rc = run_launch(c, d_seq, tab, a1, bp, unit_pair, hb, first_stores, R1, pbest, &ms1);
+        int rc = run_launch(c, d_seq, tab, a1, bp, unit_pair, hb, first_stores, R1, pbest, &ms1, true);
         if (rc != SWB_OK) return rc;
         launches += 2;
     }
@@ -1071,7 +1118,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
             b2.scols = (int2 *)c->b_scols.p;
             std::vector<BestRec> pb2;
             float ms2 = 0.f;
-            rc = run_launch(c, d_seq, tab, b2, bpw, up2, hb2, true, kBatchR, pb2, &ms2);
+            rc = run_launch(c, d_seq, tab, b2, bpw, up2, hb2, true, kBatchR, pb2, &ms2, true);
             if (rc != SWB_OK) return rc;
             launches += 2;
             for (size_t k = 0; k < tr.size(); ++k) {
