@@ -9,6 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 from dataclasses import dataclass, field
+from collections.abc import Sequence as _Seq
 from typing import List, Optional, Tuple
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -204,7 +205,7 @@ class Alignment:
     stage2_ms: float
     total_ms: float
     ops: str = ""
-    xpoints: List[Tuple[int, int, int, int]] = field(default_factory=list)  # (row, col, score, gap)
+    xpoints: "_Seq" = field(default_factory=list)  # (row, col, score, gap) tuples, built on access
     xpoint_interval: int = 0
     special_interval: int = 0
     special_bytes: int = 0
@@ -285,20 +286,6 @@ def _xpoint_array(ptr, count: int):
     return np.frombuffer(C.string_at(C.cast(ptr, C.c_void_p).value, count * size), dtype=dt)
 
 
-def _xpoint_tuples(ptr, first: int, count: int) -> list:
-    """(row, col, score, gap) tuples of count XPoint records starting at ptr[first]."""
-    if count <= 0 or not ptr:
-        return []
-    import numpy as np
-    size = C.sizeof(XPoint)
-    raw = C.string_at(C.cast(ptr, C.c_void_p).value + first * size, count * size)
-    # the records' fields viewed in (row, col, score, gap) order: tolist() builds the tuples
-    dt = np.dtype({"names": ["row", "col", "score", "gap"], "formats": [np.int64, np.int64, np.int32, np.int32],
-                   "offsets": [XPoint.row.offset, XPoint.col.offset, XPoint.score.offset, XPoint.gap.offset],
-                   "itemsize": size})
-    return np.frombuffer(raw, dtype=dt).tolist()
-
-
 class _PairXpoints:
     """Per-pair crosspoint lists of a batch, built on access: xp[i] is the list of
     (row, col, score, gap) tuples of pair i (() for pairs that were not traced).
@@ -325,9 +312,41 @@ class _PairXpoints:
         return len(self) == len(other) and all(x == y for x, y in zip(self, other))
 
 
+class _Xpoints(_Seq):
+    """A pair's crosspoints, (row, col, score, gap) tuples built on first access:
+    the records are copied to the host with the result, but 40,000 crosspoints
+    (the 1 Mbp pair) took 10 ms to turn into tuples, time the GPU sat idle
+    between alignments.  Compares equal to any sequence of the same tuples."""
+
+    def __init__(self, arr):
+        self._arr, self._list = arr, None
+
+    def _tuples(self) -> list:
+        if self._list is None:
+            self._list = self._arr.tolist() if self._arr is not None else []
+        return self._list
+
+    def __len__(self):
+        return len(self._arr) if self._arr is not None else 0
+
+    def __getitem__(self, i):
+        return self._tuples()[i]
+
+    def __iter__(self):
+        return iter(self._tuples())
+
+    def __eq__(self, other):
+        if isinstance(other, _Xpoints):
+            other = other._tuples()
+        return isinstance(other, _Seq) and self._tuples() == list(other)
+
+    def __repr__(self):
+        return repr(self._tuples())
+
+
 def _convert(r: Result) -> Alignment:
     ops = C.string_at(r.ops, r.n_ops).decode() if r.n_ops > 0 and r.ops else ""
-    xps = _xpoint_tuples(r.xpoints, 0, r.n_xpoints)
+    xps = _Xpoints(_xpoint_array(r.xpoints, r.n_xpoints) if r.n_xpoints > 0 and r.xpoints else None)
     return Alignment(r.score, r.end_row, r.end_col, r.start_row, r.start_col, bool(r.swapped),
                      r.rows, r.cols, r.stage1_ms, r.stage2_ms, r.total_ms, ops, xps,
                      r.xpoint_interval, r.special_interval, r.special_bytes, r.kernel_launches,
