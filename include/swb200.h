@@ -33,7 +33,7 @@ extern "C" {
 #define SWB_ENOMEM_BUDGET 3  /* request does not fit the context's HBM budget     */
 #define SWB_ETIMEOUT      4  /* a bounded device wait ran out                      */
 #define SWB_ECUDA         5  /* CUDA runtime error (the reference exits -2)        */
-#define SWB_EUNSUPPORTED  6  /* size or option outside what this build supports   */
+#define SWB_EUNSUPPORTED  6  /* size or option outside what this library supports */
 #define SWB_EBUSY         7  /* queue full / request slot unavailable              */
 #define SWB_ENOTFOUND     8  /* unknown request id                                 */
 

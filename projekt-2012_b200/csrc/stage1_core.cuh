@@ -2,7 +2,7 @@
 // kernel (stage1.cu) and the batched kernel (batch.cu).
 //
 // Follows the recurrence of the reference's shortPhase/longPhase kernels
-// (src/FindAlignment.cuh:50-104, twin :187-241) with this build's own layout: a
+// (src/FindAlignment.cuh:50-104, twin :187-241) with this library's own layout: a
 // warp owns a strip of 32*R rows, lane l owns R consecutive rows and computes
 // column k - l at step k; see stage1.cu for the full description.
 //

@@ -3,13 +3,13 @@
 // Replaces the reference's stage 2 (src/Crosspointer.cpp:104-338 with the
 // reverse kernels of src/TraceBack.cuh:7-472 and the host join of
 // src/SWutils.cpp:175-231).  The reference searches backwards for crosspoints
-// on its special rows; its search hangs or exits on most inputs, so this build
+// on its special rows; its search hangs or exits on most inputs, so this library
 // defines the path directly: the traceback of the forward matrix from the end
 // cell with a fixed precedence (in H: diagonal > E (column base against a gap)
 // > F (row base against a gap); in E or F: extend > open), and reports the
 // reference's crosspoints (the path's last cell on every row X with
 // (X + 1) % (4T) == 0, src/Builders.cpp:16) along that path.  The path does not
-// depend on any tuning parameter of this build.
+// depend on any tuning parameter of this library.
 //
 // How: stage 1 keeps special rows (H, F) at every strip bottom (every 448 or 512
 // rows, the strip height) and special columns (H, E) every 256 columns, so every

@@ -1,6 +1,6 @@
 """The multi-GPU column-chunk chain for one long pair (swb200/chain.py).
 
-Runs with one GPU per process in production; this build's runs have one GPU, so
+Runs with one GPU per process in production; the GPU tests get one GPU, so
 the protocol is checked on the CPU: the oracle's block function (orc_block)
 stands in for swb_score_block_device, in one process (virtual ranks) and as 2
 and 3 gloo ranks in subprocesses exchanging borders by point-to-point
