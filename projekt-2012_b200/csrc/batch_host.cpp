@@ -287,15 +287,35 @@ int32_t packed_whole_strips() {
     return -1;
 }
 
-// The packed scoring pass over the positions `pos` of `order` with R rows per
-// lane: pairs sorted by strip count and width and taken two at a time (a pair
-// whose neighbour has another strip count gets an empty partner).  Fills
-// pbest[k] for every k in pos and appends to `redo` the positions whose pair
-// reached the 16-bit limit.
-int run_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &info,
-               const std::vector<int64_t> &order, std::vector<int64_t> pos, uint32_t flags, int R,
-               std::vector<BestRec> &pbest, std::vector<int64_t> &redo, float *ms) {
-    cudaError_t e;
+// Positions of `order` whose pair may run packed (its best score is bounded
+// below the 16-bit limit, or the test flag packs every pair) and the others.
+void split_packable(const std::vector<PairInfo> &info, const std::vector<int64_t> &order, const swb_scoring *sc,
+                    uint32_t flags, std::vector<int64_t> &ppos, std::vector<int64_t> &rest) {
+    for (size_t k = 0; k < order.size(); ++k) {
+        const PairInfo &p = info[(size_t)order[k]];
+        const bool fits = (int64_t)sc->match * p.n + 256 <= kSatLimit;
+        if (fits || (flags & SWB_FLAG_TEST_PACK_ANY)) ppos.push_back((int64_t)k);
+        else rest.push_back((int64_t)k);
+    }
+}
+
+// The host half of a packed pass (see layout_packed).
+struct PackedLayout {
+    int R = 0;                    // rows per lane it was laid out for (0: none)
+    std::vector<int64_t> pos;     // the positions of `order` it covers, as given
+    std::vector<PackedPair> pp;   // packed pairs
+    std::vector<int2> up;         // work items (packed pair, strip)
+    int64_t units = 0, hb = 0;    // strips (best records) and hand-off entries
+};
+
+// The host half of the packed pass over the positions `pos` of `order` with R
+// rows per lane: pairs sorted by strip count and width and taken two at a time
+// (a pair whose neighbour has another strip count gets an empty partner), each
+// packed pair whole or chained, and the work items in their claim order.
+void layout_packed(swb_ctx *c, const std::vector<PairInfo> &info, const std::vector<int64_t> &order,
+                   std::vector<int64_t> pos, uint32_t flags, int R, PackedLayout &L) {
+    L.R = R;
+    L.pos = pos;
     const int64_t H = 32LL * R;
     const int32_t whole_max = packed_whole_strips();  // -1: by the cell share
     auto strips = [&](int64_t k) { return (info[(size_t)order[(size_t)k]].m + H - 1) / H; };
@@ -304,8 +324,10 @@ int run_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &i
         return ((uint64_t)strips(x) << 32) | (uint64_t)info[(size_t)order[(size_t)x]].n;
     });
     const int32_t dummy = (int32_t)order.size();  // slot of an empty half
-    std::vector<PackedPair> pp;
-    std::vector<int2> up;  // work items
+    std::vector<PackedPair> &pp = L.pp;
+    std::vector<int2> &up = L.up;  // work items
+    pp.clear();
+    up.clear();
     int64_t units = 0, hb = 0;
     for (size_t i = 0; i < pos.size();) {
         const int64_t ka = pos[i];
@@ -383,6 +405,28 @@ int run_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &i
             up.push_back(make_int2(flow[i], s));
     for (size_t q = 0; q < pp.size(); ++q)
         if (pp[q].whole) up.push_back(make_int2((int32_t)q, 0));
+    L.units = units;
+    L.hb = hb;
+}
+
+// The packed scoring pass over the positions `pos` of `order` with R rows per
+// lane (the layout `pre` when it was made for the same R and positions).  Fills
+// pbest[k] for every k in pos and appends to `redo` the positions whose pair
+// reached the 16-bit limit.
+int run_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &info,
+               const std::vector<int64_t> &order, const std::vector<int64_t> &pos, uint32_t flags, int R,
+               std::vector<BestRec> &pbest, std::vector<int64_t> &redo, float *ms,
+               const PackedLayout *pre = nullptr) {
+    cudaError_t e;
+    PackedLayout local;
+    const PackedLayout *L = pre;
+    if (!L || L->R != R || L->pos != pos) {
+        layout_packed(c, info, order, pos, flags, R, local);
+        L = &local;
+    }
+    const std::vector<PackedPair> &pp = L->pp;
+    const std::vector<int2> &up = L->up;
+    const int64_t units = L->units, hb = L->hb;
     const int64_t np = (int64_t)pp.size(), nslots = (int64_t)order.size() + 1, items = (int64_t)up.size();
     const size_t pp_bytes = sizeof(PackedPair) * (size_t)np, up_bytes = sizeof(int2) * (size_t)items;
     const size_t back = sizeof(BestRec) * (size_t)nslots + sizeof(int32_t) * (size_t)nslots + 64;
@@ -458,21 +502,20 @@ constexpr int64_t kTuneMinPairs = 16384;
 // eighth of the batch each, the same length mix), those results are kept and
 // their positions leave ppos, and the candidate with the most cells per ms is
 // recorded.  Batches below kTuneMinPairs take kBatch16R.
-int tune_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &info,
-                const std::vector<int64_t> &order, std::vector<int64_t> &ppos, uint32_t flags,
-                std::vector<BestRec> &pbest, std::vector<int64_t> &redo, float *ms, int32_t *launches, int *R,
-                const char **how) {
-    *R = kBatch16R;
-    *how = "default";
+// Rows per lane of the packed pass over ppos when no probe is needed:
+// SWB_BATCH16_R, the recorded choice of the batch's bucket, or kBatch16R for
+// batches too small to probe; 0 when the bucket is new and the batch large.
+int packed_rows_known(swb_ctx *c, const std::vector<PairInfo> &info, const std::vector<int64_t> &order,
+                      const std::vector<int64_t> &ppos, const char **how, std::string *key_out) {
     if (const char *v = std::getenv("SWB_BATCH16_R")) {
         const int r = std::atoi(v);
         if (r == kBatch16R || r == kBatch16RShort) {
-            *R = r;
             *how = "SWB_BATCH16_R";
-            return SWB_OK;
+            return r;
         }
     }
-    if (ppos.empty()) return SWB_OK;
+    *how = "default";
+    if (ppos.empty()) return kBatch16R;
     // ceil(log2) of the cells-weighted median rows and columns of the packed
     // pairs: the median's power-of-two bucket, from per-bucket cell sums
     auto median = [&](bool rows) {
@@ -492,13 +535,23 @@ int tune_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &
         return (int64_t)1 << 62;
     };
     const std::string key = batch_tune_key(c->sms, "batch16", median(true), median(false));
+    if (key_out) *key_out = key;
     int cached = 0;
     if (tune_lookup(key, &cached) && (cached == kBatch16R || cached == kBatch16RShort)) {
-        *R = cached;
         *how = "cached";
-        return SWB_OK;
+        return cached;
     }
-    if ((int64_t)ppos.size() < kTuneMinPairs) return SWB_OK;
+    return (int64_t)ppos.size() < kTuneMinPairs ? kBatch16R : 0;
+}
+
+int tune_packed(swb_ctx *c, const BatchArgs &base, const std::vector<PairInfo> &info,
+                const std::vector<int64_t> &order, std::vector<int64_t> &ppos, uint32_t flags,
+                std::vector<BestRec> &pbest, std::vector<int64_t> &redo, float *ms, int32_t *launches, int *R,
+                const char **how) {
+    std::string key;
+    const int known = packed_rows_known(c, info, order, ppos, how, &key);
+    *R = known > 0 ? known : kBatch16R;
+    if (known > 0) return SWB_OK;
     const int cands[2] = {kBatch16R, kBatch16RShort};
     double rate[2] = {0.0, 0.0};
     for (int i = 0; i < 2; ++i) {
@@ -940,6 +993,20 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
         ph.mark("sequences to the device");
     }
 
+    // The packed pass's host layout (sorting, packing, claim order: several ms
+    // for 100,000 pairs) is built now, while the sequences are still on their
+    // way to the device, whenever its strip height needs no probe.  If the
+    // batch then turns out not to be in the table mode, it goes unused.
+    PackedLayout early;
+    if (pack_candidate && !order.empty() && !use_graph) {
+        std::vector<int64_t> ppos, rest;
+        split_packable(info, order, sc, flags, ppos, rest);
+        const char *how = "";
+        const int R = packed_rows_known(c, info, order, ppos, &how, nullptr);
+        if (R > 0 && !ppos.empty()) layout_packed(c, info, order, ppos, flags, R, early);
+        ph.mark("packed layout");
+    }
+
     BatchArgs base{};
     base.wait_limit = c->wait_cycles;
     base.open = sc->gap_open;
@@ -1011,12 +1078,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
         // pairs whose best score is bounded below the 16-bit limit run packed two
         // per warp; the others, and any pair that reached the limit, in int32
         std::vector<int64_t> ppos, rest;
-        for (size_t k = 0; k < order.size(); ++k) {
-            const PairInfo &p = info[(size_t)order[k]];
-            const bool fits = (int64_t)sc->match * p.n + 256 <= 32767 - 256;
-            if (fits || (flags & SWB_FLAG_TEST_PACK_ANY)) ppos.push_back((int64_t)k);
-            else rest.push_back((int64_t)k);
-        }
+        split_packable(info, order, sc, flags, ppos, rest);
         pbest.assign(order.size(), BestRec{});
         int Rp = kBatch16R;
         const char *how = "";
@@ -1024,7 +1086,7 @@ int batch_run(swb_ctx *c, const uint8_t *h_seq, const uint8_t *d_seq_in, int64_t
         if (rc != SWB_OK) return rc;
         if (ph.on) std::fprintf(stderr, "swb batch: packed rows per lane %d (%s)\n", Rp, how);
         if (!ppos.empty()) {
-            rc = run_packed(c, base, info, order, ppos, flags, Rp, pbest, rest, &ms1);
+            rc = run_packed(c, base, info, order, ppos, flags, Rp, pbest, rest, &ms1, &early);
             if (rc != SWB_OK) return rc;
             launches += 2;
         }
